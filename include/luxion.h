@@ -1,0 +1,300 @@
+/*
+ * luxion.h -- C-ABI of the B200 wavefront path tracer.
+ *
+ * The entry points replace the render path of seabiscuit-iv/luxion:
+ *   pathtraceInit(Scene*)         include/pathtrace/pathtrace_buffers.h:5,
+ *                                 src/pathtrace/pathtrace_buffers.cu:21-140   -> lux_init
+ *   pathtrace(uchar4*, int, int)  include/pathtrace.h:13, src/pathtrace.cu:97  -> lux_render_iter
+ *   pathtraceFree()               include/pathtrace/pathtrace_buffers.h:6,
+ *                                 src/pathtrace/pathtrace_buffers.cu:142-177  -> lux_free
+ *   copyImageToHost()             include/pathtrace/pathtrace_buffers.h:7,
+ *                                 src/pathtrace/pathtrace_buffers.cu:180-190  -> lux_copy_image
+ *   PathTracerOptions             include/pathtrace/pathtracer_options.h:3-21 -> lux_options
+ *   checkCUDAError (exit on error) include/common.h:16-36                    -> status codes +
+ *                                                                              lux_last_error
+ *
+ * Conventions: plain C types only; every call returns LUX_OK (0) or a negative status and
+ * never exits the process.  The caller owns every host buffer it passes; a context owns its
+ * device memory.  A context is used by one host thread at a time; distinct contexts may run
+ * concurrently on distinct streams.
+ */
+#ifndef LUXION_H
+#define LUXION_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LUX_ABI_VERSION 1
+
+/* ---- status codes ---------------------------------------------------------------------- */
+enum {
+    LUX_OK = 0,
+    LUX_ERR_INVALID = -1,     /* bad argument or malformed scene                           */
+    LUX_ERR_CUDA = -2,        /* a CUDA runtime call failed (text in lux_last_error)        */
+    LUX_ERR_NO_DEVICE = -3,   /* no sm_100 device visible                                  */
+    LUX_ERR_OOM = -4,         /* device allocation failed or the HBM budget is exceeded    */
+    LUX_ERR_UNSUPPORTED = -5, /* option combination not implemented                        */
+    LUX_ERR_TIMEOUT = -6,     /* a bounded device wait gave up (status read from device)   */
+    LUX_ERR_STATE = -7        /* call out of order (e.g. render before init)               */
+};
+
+/* ---- scene description (POD views of caller-owned host memory) ------------------------- */
+
+/* Texel storage formats. The reference stores every texture as float4 with hardware
+ * bilinear filtering, wrap addressing and normalised coordinates (src/texture.cu:12-69). */
+enum {
+    LUX_TEX_RGBA8 = 0,    /* 4 x u8 unorm                    */
+    LUX_TEX_RGBA16 = 1,   /* 4 x u16 unorm                   */
+    LUX_TEX_RGBA32F = 2,  /* 4 x f32                         */
+    LUX_TEX_RGBA16F = 3   /* 4 x f16 (IEEE binary16)         */
+};
+
+typedef struct lux_texture_desc {
+    int32_t width, height;
+    int32_t format;          /* LUX_TEX_*                                                   */
+    int32_t _pad;
+    const void* data;        /* width*height texels, row-major, 4 channels                  */
+} lux_texture_desc;
+
+/* KHR_texture_transform: uv*scale -> rotate -> +offset (src/material_queries.cu:3-17). */
+typedef struct lux_tex_transform {
+    float offset[2];
+    float scale[2];
+    float rotation;
+} lux_tex_transform;
+
+enum { LUX_ALPHA_OPAQUE = 0, LUX_ALPHA_MASK = 1, LUX_ALPHA_BLEND = 2 };
+
+/* Mirrors the fields of the reference Material the uber-shader reads
+ * (include/sceneStructs.h:94-131). Texture indices are -1 when absent. */
+typedef struct lux_material_desc {
+    float color[3];
+    int32_t albedo_tex;
+    float alpha;
+    int32_t alpha_mode;      /* LUX_ALPHA_*                                                 */
+    float alpha_cutoff;
+    float emission_strength;
+    float emission_color[3];
+    int32_t emissive_tex;
+    float roughness;
+    float metallic;
+    int32_t normal_tex;
+    int32_t metallic_roughness_tex;
+    float transmission;
+    float ior;
+    lux_tex_transform albedo_tt, emissive_tt, normal_tt, metallic_roughness_tt;
+} lux_material_desc;
+
+/* One triangle mesh in object space. A single index stream addresses positions, normals and
+ * uvs, as the reference's glTF loader does (src/scene/scene_load_gltf.cpp:430). */
+typedef struct lux_mesh_desc {
+    int32_t num_verts;
+    int32_t num_tris;
+    const float* positions;  /* num_verts * 3                                               */
+    const float* normals;    /* num_verts * 3, or NULL (geometric normals are used)          */
+    const float* uvs;        /* num_verts * 2, or NULL (uv = 0, tangent = +x)                */
+    const uint32_t* indices; /* num_tris * 3                                                */
+} lux_mesh_desc;
+
+/* One placed mesh (a reference Geom, include/sceneStructs.h:66-79). Matrices are 4x4
+ * column-major, the glm layout. When has_inverse is 0 the library derives inverse and
+ * inverse-transpose itself. */
+typedef struct lux_instance_desc {
+    int32_t mesh;
+    int32_t material;
+    int32_t has_inverse;
+    int32_t _pad;
+    float transform[16];
+    float inverse[16];
+    float inv_transpose[16];
+} lux_instance_desc;
+
+/* Pinhole camera, the reference Camera (include/sceneStructs.h:133-143). */
+typedef struct lux_camera_desc {
+    int32_t width, height;
+    float position[3];
+    float look_at[3];
+    float view[3];
+    float up[3];
+    float right[3];
+    float fov[2];
+    float pixel_length[2];
+} lux_camera_desc;
+
+typedef struct lux_scene_desc {
+    int32_t num_meshes, num_instances, num_materials, num_textures;
+    const lux_mesh_desc* meshes;
+    const lux_instance_desc* instances;
+    const lux_material_desc* materials;
+    const lux_texture_desc* textures;
+    lux_camera_desc camera;
+    int32_t trace_depth;     /* RenderState::traceDepth (include/sceneStructs.h:145-151)      */
+    /* Environment map (an HDRI); env_data NULL means none. RGBA texels; the reference keeps
+     * the alpha channel and feeds it to the CDF weight (src/scene/scene_precompute.cpp:88). */
+    int32_t env_width, env_height;
+    int32_t env_format;      /* LUX_TEX_RGBA32F or LUX_TEX_RGBA16F                          */
+    const void* env_data;
+} lux_scene_desc;
+
+/* ---- options (PathTracerOptions + CLI flags -dmis -emis) -------------------------------- */
+enum { LUX_TONEMAP_REINHARD = 0, LUX_TONEMAP_AGX = 1, LUX_TONEMAP_ACES = 2 };
+enum { LUX_PRECISION_PLAIN = 0, LUX_PRECISION_COMPENSATED = 1 };
+
+typedef struct lux_options {
+    int32_t direct_light_sampling;       /* -dmis                                            */
+    int32_t env_importance_sampling;     /* -emis                                            */
+    int32_t color_mode;                  /* LUX_TONEMAP_*, default ACES                       */
+    float envmap_intensity;              /* default 1                                        */
+    int32_t trace_depth;                 /* 0: take scene trace_depth                        */
+    int32_t ray_sorting;                 /* 1: Morton-sort each bounce's queue (RAY_SORTING)  */
+    int32_t precision;                   /* LUX_PRECISION_*                                  */
+    int32_t spp_per_wave;                /* samples kept in flight together; 0 = automatic    */
+    int32_t use_graph;                   /* 1: replay the bounce loop as a CUDA graph         */
+    int32_t device;                      /* CUDA device ordinal                              */
+    void* stream;                        /* cudaStream_t to launch on; NULL = a private one  */
+} lux_options;
+
+typedef struct lux_ctx lux_ctx;
+
+/* Fill *opt with the reference defaults (include/pathtrace/pathtracer_options.h:3-11). */
+void lux_default_options(lux_options* opt);
+
+/* pathtraceInit: upload the scene, build the acceleration structure and the light CDFs,
+ * allocate every per-path buffer. */
+int lux_init(const lux_scene_desc* scene, const lux_options* opt, lux_ctx** out);
+
+/* pathtrace: render one sample per pixel. iter is 1-based and seeds the RNG exactly like
+ * the reference (include/common.h:38-47). The sample is added to the FP32 accumulation
+ * image. If rgba8_dev is not NULL it receives the tonemapped image of the running mean
+ * (sendImageToPBO, src/kernels/image_kernels.cu:6-46); it is a device pointer, as the
+ * reference's PBO is. */
+int lux_render_iter(lux_ctx* ctx, int iter, uint8_t* rgba8_dev);
+
+/* Render n_iter samples, iterations first_iter .. first_iter+n_iter-1, keeping up to
+ * spp_per_wave of them in flight together; the image equals n_iter lux_render_iter calls. */
+int lux_render(lux_ctx* ctx, int first_iter, int n_iter);
+
+/* copyImageToHost: the accumulation SUM (not the mean), W*H*3 floats. */
+int lux_copy_image(lux_ctx* ctx, float* rgb_host);
+
+/* Tonemapped RGBA8 of the running mean into a host buffer (W*H*4 bytes). */
+int lux_copy_rgba8(lux_ctx* ctx, uint8_t* rgba_host);
+
+/* Zero the accumulation image (the reference re-inits on camera change,
+ * src/app/render_loop.cpp:122-126). */
+int lux_reset(lux_ctx* ctx);
+
+/* Replace the camera of a live context (same resolution) and zero the image. */
+int lux_set_camera(lux_ctx* ctx, const lux_camera_desc* cam);
+
+/* pathtraceFree: release everything; NULL is accepted (idempotent, like the reference). */
+int lux_free(lux_ctx* ctx);
+
+/* Thread-local text of the last failing call. */
+const char* lux_last_error(void);
+
+/* ---- statistics of the last lux_render / lux_render_iter call --------------------------- */
+typedef struct lux_stats {
+    double rays_radiance;     /* radiance rays traced                                        */
+    double rays_shadow;       /* NEE shadow rays traced (DL + env)                           */
+    double path_bounces;      /* queue entries shaded                                        */
+    double samples;           /* pixel-samples rendered                                      */
+    double ms_total;          /* device time of the call (CUDA events)                       */
+    double ms_trace;          /* summed device time of the trace kernels                     */
+    double ms_shade;          /* summed device time of the shade kernels                     */
+    double ms_camera;         /* summed device time of camera generation                     */
+    double ms_accum;          /* summed device time of accumulation                          */
+    double ms_sort;           /* summed device time of Morton keys + sort                    */
+    double launches_trace, launches_shade, launches_camera, launches_accum, launches_sort;
+    double kernel_launches;   /* every kernel this library launched in the call              */
+} lux_stats;
+
+/* Per-kernel CUDA-event timing is recorded only while enabled (off by default). */
+int lux_enable_timing(lux_ctx* ctx, int on);
+int lux_get_stats(lux_ctx* ctx, lux_stats* out);
+
+/* ---- kernel-level entry points used by the parity suite --------------------------------- */
+
+/* Closest-hit / any-hit trace of caller rays through the device BVH.
+ * rays: n * 8 floats (origin xyz, tmax, direction xyz, pixel-as-float-bits).
+ * mode 0: closest hit (radiance; pixel and iter key the alpha-blend hash);
+ * mode 1: closest hit with tmax (DL shadow); mode 2: any hit (env shadow).
+ * hits: n * 5 words (t as f32 bits, instance, prim, u bits, v bits); t=-1 on a miss; for
+ * mode 2 only word 0 is meaningful (1.0 occluded, -1.0 free). Host buffers. */
+int lux_trace_rays(lux_ctx* ctx, const float* rays, int n, int mode, int iter, uint32_t* hits);
+
+/* Morton keys of caller rays (src/morton_codes.cu:13-24, src/kernels/intersection_precompute.cu:6-33):
+ * rays as in lux_trace_rays; keys: n u32. Host buffers. */
+int lux_morton_keys(lux_ctx* ctx, const float* rays, int n, uint32_t* keys);
+
+/* One bounce of the wavefront on caller state, for the shade parity test. The caller gives
+ * n paths (path state, 24 floats each, layout LUX_PS_*) and the traced hits for them
+ * (10 words each: radiance hit, then shadow hit / occlusion), the bounce depth after the
+ * increment, and whether compaction is on. The kernel updates the states in place and
+ * writes the survivor path indices; *n_out receives their number. Host buffers. */
+enum {
+    LUX_PS_ORIGIN = 0, LUX_PS_DIR = 3, LUX_PS_COLOR = 6, LUX_PS_THROUGHPUT = 9,
+    LUX_PS_DL = 12, LUX_PS_ENV = 15, LUX_PS_PIXEL = 18, LUX_PS_KILL = 19,
+    LUX_PS_SPECULAR = 20, LUX_PS_LAST_PDF = 21, LUX_PS_FLOATS = 24
+};
+int lux_shade_step(lux_ctx* ctx, int iter, int depth, int compact, float* paths, int n,
+                   const uint32_t* hits, int* survivors, int* n_out);
+
+/* Light samples (sampleDirectLight, src/kernels/sample_direct_light.cu:9-101) for n paths of
+ * the given pixels at bounce depth: out n*6 floats (DL point xyz, env dir xyz). */
+int lux_light_samples(lux_ctx* ctx, int iter, int depth, const int* pixels, int n, float* out);
+
+/* Light-CDF tables as built on the device side (emissive prefix, per-mesh triangle prefix of
+ * each emissive instance concatenated, HDRI marginal, HDRI conditional), for CDF parity. */
+int lux_get_cdfs(lux_ctx* ctx, float* emissive_prefix, float* tri_prefix, float* marginal,
+                 float* conditional, float* total_area);
+
+/* Device-side minstd stream: n uniforms of the engine seeded by (iter, index, depth)
+ * into a host buffer, for RNG parity. */
+int lux_rng_stream(int iter, int index, int depth, int n, float* out);
+
+/* Bilinear texture fetches of a scene texture (index -1: the environment map) at n (u, v)
+ * pairs; out n*4 floats. */
+int lux_sample_texture(lux_ctx* ctx, int tex, const float* uv, int n, float* out);
+
+/* ---- procedural scenes (host only; no device needed) ------------------------------------ */
+typedef struct lux_host_scene lux_host_scene;
+
+/* Cornell box, 36 triangles, 256x256 (the 36-triangle config of the baseline). */
+lux_host_scene* lux_scene_cornell36(int width, int height);
+
+/* Random instanced scene: num_instances icospheres / displaced grids with total_tris
+ * triangles, random materials, value-noise textures and an HDRI; seeded. */
+typedef struct lux_random_scene_params {
+    uint64_t seed;
+    int32_t num_instances;
+    int32_t total_tris;
+    int32_t min_tris, max_tris;
+    int32_t num_emissive;
+    int32_t num_textures;
+    int32_t texture_size;
+    int32_t env_width, env_height;   /* 0 for no HDRI                                       */
+    int32_t width, height;
+    int32_t trace_depth;
+    int32_t env_half;                /* 1: store the HDRI as RGBA16F                         */
+    int32_t tex_half;                /* 1: store base-colour textures as RGBA16F             */
+} lux_random_scene_params;
+void lux_default_random_scene_params(lux_random_scene_params* p);
+lux_host_scene* lux_scene_random(const lux_random_scene_params* p);
+
+/* Furnace: a closed unit sphere (Lambert albedo 1) inside a constant environment of 1. */
+lux_host_scene* lux_scene_furnace(int width, int height, int subdiv);
+
+const lux_scene_desc* lux_scene_get_desc(const lux_host_scene* s);
+/* Total triangles over all instances. */
+int64_t lux_scene_instanced_tris(const lux_host_scene* s);
+void lux_scene_destroy(lux_host_scene* s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LUXION_H */
