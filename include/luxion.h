@@ -143,6 +143,11 @@ typedef struct lux_scene_desc {
 /* ---- options (PathTracerOptions + CLI flags -dmis -emis) -------------------------------- */
 enum { LUX_TONEMAP_REINHARD = 0, LUX_TONEMAP_AGX = 1, LUX_TONEMAP_ACES = 2 };
 enum { LUX_PRECISION_PLAIN = 0, LUX_PRECISION_COMPENSATED = 1 };
+/* How scene textures are held in HBM. FLOAT converts 8/16-bit texels to float4 exactly as
+ * the reference's upload does (src/texture.cu:17-27), so filtered values match it; UNORM8
+ * keeps 8-bit texels as they are (4 B/texel, filtered by the hardware unorm path); HALF
+ * stores IEEE binary16 (the precision form). */
+enum { LUX_TEXSTORE_FLOAT = 0, LUX_TEXSTORE_UNORM8 = 1, LUX_TEXSTORE_HALF = 2 };
 
 typedef struct lux_options {
     int32_t direct_light_sampling;       /* -dmis                                            */
@@ -154,6 +159,7 @@ typedef struct lux_options {
     int32_t precision;                   /* LUX_PRECISION_*                                  */
     int32_t spp_per_wave;                /* samples kept in flight together; 0 = automatic    */
     int32_t use_graph;                   /* 1: replay the bounce loop as a CUDA graph         */
+    int32_t texture_storage;             /* LUX_TEXSTORE_*                                    */
     int32_t device;                      /* CUDA device ordinal                              */
     void* stream;                        /* cudaStream_t to launch on; NULL = a private one  */
 } lux_options;

@@ -1,0 +1,319 @@
+"""luxion_b200 -- B200-native wavefront path tracer behind the luxion render-path interface.
+
+The product is the C-ABI library ``_lib/libluxion.so`` (include/luxion.h). This module is a
+thin ctypes mirror of the reference's host interface for the render path:
+
+    pathtraceInit(scene)      include/pathtrace/pathtrace_buffers.h:5
+    pathtrace(pbo, frame, it) include/pathtrace.h:13
+    pathtraceFree()           include/pathtrace/pathtrace_buffers.h:6
+    copyImageToHost()         include/pathtrace/pathtrace_buffers.h:7
+    PathTracerOptions         include/pathtrace/pathtracer_options.h:3-21
+
+plus an object API (``Renderer``) for callers that want several contexts. Every call goes
+through the CUDA library; there is no CPU fallback: when the library is missing or no
+sm_100 device is visible the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+from . import _ffi
+from ._ffi import (CameraDesc, Options, RandomSceneParams, SceneDesc, Stats, c_float_p, c_int_p,
+                   c_u32_p, default_options)
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libluxion.so")
+_lib: Optional[C.CDLL] = None
+
+# every symbol include/luxion.h declares, with its ctypes signature
+_P = C.c_void_p
+SIGNATURES = {
+    "lux_default_options": (None, [C.POINTER(Options)]),
+    "lux_init": (C.c_int, [C.POINTER(SceneDesc), C.POINTER(Options), C.POINTER(_P)]),
+    "lux_render_iter": (C.c_int, [_P, C.c_int, _P]),
+    "lux_render": (C.c_int, [_P, C.c_int, C.c_int]),
+    "lux_copy_image": (C.c_int, [_P, c_float_p]),
+    "lux_copy_rgba8": (C.c_int, [_P, C.POINTER(C.c_uint8)]),
+    "lux_reset": (C.c_int, [_P]),
+    "lux_set_camera": (C.c_int, [_P, C.POINTER(CameraDesc)]),
+    "lux_free": (C.c_int, [_P]),
+    "lux_last_error": (C.c_char_p, []),
+    "lux_enable_timing": (C.c_int, [_P, C.c_int]),
+    "lux_get_stats": (C.c_int, [_P, C.POINTER(Stats)]),
+    "lux_trace_rays": (C.c_int, [_P, c_float_p, C.c_int, C.c_int, C.c_int, c_u32_p]),
+    "lux_morton_keys": (C.c_int, [_P, c_float_p, C.c_int, c_u32_p]),
+    "lux_shade_step": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, c_float_p, C.c_int, c_u32_p, c_int_p, c_int_p]),
+    "lux_light_samples": (C.c_int, [_P, C.c_int, C.c_int, c_int_p, C.c_int, c_float_p]),
+    "lux_get_cdfs": (C.c_int, [_P, c_float_p, c_float_p, c_float_p, c_float_p, c_float_p]),
+    "lux_rng_stream": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, c_float_p]),
+    "lux_sample_texture": (C.c_int, [_P, C.c_int, c_float_p, C.c_int, c_float_p]),
+    "lux_scene_cornell36": (_P, [C.c_int, C.c_int]),
+    "lux_default_random_scene_params": (None, [C.POINTER(RandomSceneParams)]),
+    "lux_scene_random": (_P, [C.POINTER(RandomSceneParams)]),
+    "lux_scene_furnace": (_P, [C.c_int, C.c_int, C.c_int]),
+    "lux_scene_get_desc": (C.POINTER(SceneDesc), [_P]),
+    "lux_scene_instanced_tris": (C.c_int64, [_P]),
+    "lux_scene_destroy": (None, [_P]),
+}
+
+
+class LuxError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{_ffi.STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def lib() -> C.CDLL:
+    """Load the CUDA library (building it first if the sources are newer)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        from . import build as _build
+        _build.build()
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"luxion CUDA library missing: {LIB_PATH}")
+    L = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise LuxError(rc, lib().lux_last_error().decode(errors="replace"))
+
+
+def ptr(a: np.ndarray, t=C.c_float):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+# ---- procedural scenes (host only) ---------------------------------------------------------
+class HostScene:
+    """Host-side scene description produced by the library's procedural generators."""
+
+    def __init__(self, handle):
+        if not handle:
+            raise LuxError(-1, "scene generation failed")
+        self._h = handle
+
+    @property
+    def desc(self) -> SceneDesc:
+        return lib().lux_scene_get_desc(self._h).contents
+
+    @property
+    def desc_ptr(self):
+        return lib().lux_scene_get_desc(self._h)
+
+    @property
+    def instanced_tris(self) -> int:
+        return int(lib().lux_scene_instanced_tris(self._h))
+
+    @property
+    def width(self) -> int:
+        return self.desc.camera.width
+
+    @property
+    def height(self) -> int:
+        return self.desc.camera.height
+
+    def close(self):
+        if self._h:
+            lib().lux_scene_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def cornell36(width: int = 256, height: int = 256) -> HostScene:
+    return HostScene(lib().lux_scene_cornell36(width, height))
+
+
+def random_scene(**kw) -> HostScene:
+    p = RandomSceneParams()
+    lib().lux_default_random_scene_params(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return HostScene(lib().lux_scene_random(C.byref(p)))
+
+
+def furnace(width: int = 64, height: int = 64, subdiv: int = 16) -> HostScene:
+    return HostScene(lib().lux_scene_furnace(width, height, subdiv))
+
+
+# ---- renderer -------------------------------------------------------------------------------
+class Renderer:
+    """One render context (lux_ctx): a resident scene plus its accumulation image."""
+
+    def __init__(self, scene, options: Optional[Options] = None, **kw):
+        self.scene = scene
+        self.options = options if options is not None else default_options(**kw)
+        h = C.c_void_p()
+        _check(lib().lux_init(scene.desc_ptr, C.byref(self.options), C.byref(h)))
+        self._h = h
+        self.width = scene.width
+        self.height = scene.height
+
+    def render_iter(self, it: int, rgba8_dev: int = 0):
+        _check(lib().lux_render_iter(self._h, it, C.c_void_p(rgba8_dev) if rgba8_dev else None))
+
+    def render(self, first_iter: int, n_iter: int):
+        _check(lib().lux_render(self._h, first_iter, n_iter))
+
+    def image_sum(self) -> np.ndarray:
+        out = np.empty((self.height, self.width, 3), np.float32)
+        _check(lib().lux_copy_image(self._h, ptr(out)))
+        return out
+
+    def rgba8(self) -> np.ndarray:
+        out = np.empty((self.height, self.width, 4), np.uint8)
+        _check(lib().lux_copy_rgba8(self._h, out.ctypes.data_as(C.POINTER(C.c_uint8))))
+        return out
+
+    def reset(self):
+        _check(lib().lux_reset(self._h))
+
+    def set_camera(self, cam: CameraDesc):
+        _check(lib().lux_set_camera(self._h, C.byref(cam)))
+
+    def enable_timing(self, on: bool = True):
+        _check(lib().lux_enable_timing(self._h, 1 if on else 0))
+
+    def stats(self) -> dict:
+        s = Stats()
+        _check(lib().lux_get_stats(self._h, C.byref(s)))
+        return {n: getattr(s, n) for n, _ in Stats._fields_}
+
+    # kernel-level entry points (parity suite)
+    def trace_rays(self, rays: np.ndarray, mode: int = 0, it: int = 1) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = rays.shape[0]
+        hits = np.zeros((n, 5), np.uint32)
+        _check(lib().lux_trace_rays(self._h, ptr(rays), n, mode, it, ptr(hits, C.c_uint32)))
+        return hits
+
+    def morton_keys(self, rays: np.ndarray) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, np.float32)
+        keys = np.zeros(rays.shape[0], np.uint32)
+        _check(lib().lux_morton_keys(self._h, ptr(rays), rays.shape[0], ptr(keys, C.c_uint32)))
+        return keys
+
+    def shade_step(self, paths: np.ndarray, hits: np.ndarray, it: int, depth: int, compact: int = 1):
+        paths = np.ascontiguousarray(paths, np.float32).copy()
+        hits = np.ascontiguousarray(hits, np.uint32)
+        n = paths.shape[0]
+        surv = np.zeros(max(n, 1), np.int32)
+        nout = C.c_int(0)
+        _check(lib().lux_shade_step(self._h, it, depth, compact, ptr(paths), n, ptr(hits, C.c_uint32),
+                                    ptr(surv, C.c_int), C.byref(nout)))
+        return paths, surv[: nout.value].copy()
+
+    def light_samples(self, pixels: np.ndarray, it: int, depth: int) -> np.ndarray:
+        pixels = np.ascontiguousarray(pixels, np.int32)
+        out = np.zeros((pixels.shape[0], 6), np.float32)
+        _check(lib().lux_light_samples(self._h, it, depth, ptr(pixels, C.c_int), pixels.shape[0], ptr(out)))
+        return out
+
+    def cdfs(self, sizes) -> dict:
+        ne, ntp, eh, ew = sizes
+        ep = np.zeros(max(ne, 1), np.float32)
+        tp = np.zeros(max(ntp, 1), np.float32)
+        mg = np.zeros(max(eh, 1), np.float32)
+        cd = np.zeros(max(eh * ew, 1), np.float32)
+        ta = C.c_float(0)
+        _check(lib().lux_get_cdfs(self._h, ptr(ep), ptr(tp), ptr(mg), ptr(cd), C.byref(ta)))
+        return {"emissive_prefix": ep[:ne], "tri_prefix": tp[:ntp], "marginal": mg[:eh],
+                "conditional": cd[: eh * ew], "total_area": ta.value}
+
+    def sample_texture(self, tex: int, uv: np.ndarray) -> np.ndarray:
+        uv = np.ascontiguousarray(uv, np.float32)
+        out = np.zeros((uv.shape[0], 4), np.float32)
+        _check(lib().lux_sample_texture(self._h, tex, ptr(uv), uv.shape[0], ptr(out)))
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().lux_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def rng_stream(it: int, index: int, depth: int, n: int) -> np.ndarray:
+    out = np.zeros(n, np.float32)
+    _check(lib().lux_rng_stream(it, index, depth, n, ptr(out)))
+    return out
+
+
+# ---- reference-shaped module interface --------------------------------------------------------
+class PathTracerOptions:
+    """Singleton options, as include/pathtrace/pathtracer_options.h:3-21."""
+
+    _instance: Optional["PathTracerOptions"] = None
+
+    def __init__(self):
+        self.debug_bvh = False
+        self.material_debug_mode = 0
+        self.color_mode = _ffi.TONEMAP_ACES
+        self.envmap_intensity = 1.0
+        self.direct_light_sampling = False
+        self.environment_map_importance_sampling = False
+        self.selected_material = 0
+
+    @classmethod
+    def Get(cls) -> "PathTracerOptions":
+        if cls._instance is None:
+            cls._instance = PathTracerOptions()
+        return cls._instance
+
+    def to_options(self, **kw) -> Options:
+        return default_options(direct_light_sampling=int(self.direct_light_sampling),
+                               env_importance_sampling=int(self.environment_map_importance_sampling),
+                               color_mode=int(self.color_mode), envmap_intensity=float(self.envmap_intensity), **kw)
+
+
+_state: Optional[Renderer] = None
+
+
+def pathtraceInit(scene, **kw) -> None:
+    """Allocate and upload everything for `scene` (src/pathtrace/pathtrace_buffers.cu:21-140)."""
+    global _state
+    pathtraceFree()
+    _state = Renderer(scene, PathTracerOptions.Get().to_options(**kw))
+
+
+def pathtrace(pbo: int, frame: int, iteration: int) -> None:
+    """One sample per pixel (src/pathtrace.cu:97-367). `pbo` is a device pointer or 0."""
+    del frame  # unused by the reference as well
+    if _state is None:
+        raise LuxError(-7, "pathtrace called before pathtraceInit")
+    _state.render_iter(iteration, pbo)
+
+
+def pathtraceFree() -> None:
+    global _state
+    if _state is not None:
+        _state.close()
+        _state = None
+
+
+def copyImageToHost() -> np.ndarray:
+    """The FP32 accumulation sum (src/pathtrace/pathtrace_buffers.cu:180-190)."""
+    if _state is None:
+        raise LuxError(-7, "copyImageToHost called before pathtraceInit")
+    return _state.image_sum()

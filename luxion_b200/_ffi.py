@@ -1,7 +1,7 @@
 """ctypes mirror of include/luxion.h (the C-ABI of the render path).
 
-The structures below must match the C declarations field for field; tests check their
-sizes against the library's own view (``lux_struct_sizes``).
+The structures below must match the C declarations field for field; the CPU tests check
+their sizes and offsets against a C compiler's view of the header.
 """
 from __future__ import annotations
 
@@ -27,6 +27,7 @@ TEX_RGBA8, TEX_RGBA16, TEX_RGBA32F, TEX_RGBA16F = 0, 1, 2, 3
 ALPHA_OPAQUE, ALPHA_MASK, ALPHA_BLEND = 0, 1, 2
 TONEMAP_REINHARD, TONEMAP_AGX, TONEMAP_ACES = 0, 1, 2
 PRECISION_PLAIN, PRECISION_COMPENSATED = 0, 1
+TEXSTORE_FLOAT, TEXSTORE_UNORM8, TEXSTORE_HALF = 0, 1, 2
 
 # path-state layout (LUX_PS_*)
 PS_ORIGIN, PS_DIR, PS_COLOR, PS_THROUGHPUT = 0, 3, 6, 9
@@ -85,7 +86,8 @@ class Options(C.Structure):
                 ("color_mode", C.c_int32), ("envmap_intensity", C.c_float),
                 ("trace_depth", C.c_int32), ("ray_sorting", C.c_int32),
                 ("precision", C.c_int32), ("spp_per_wave", C.c_int32),
-                ("use_graph", C.c_int32), ("device", C.c_int32), ("stream", C.c_void_p)]
+                ("use_graph", C.c_int32), ("texture_storage", C.c_int32), ("device", C.c_int32),
+                ("stream", C.c_void_p)]
 
 
 class Stats(C.Structure):
@@ -116,6 +118,7 @@ def default_options(**kw) -> Options:
     o.precision = PRECISION_PLAIN
     o.spp_per_wave = 0
     o.use_graph = 1
+    o.texture_storage = TEXSTORE_FLOAT
     o.device = 0
     o.stream = None
     for k, v in kw.items():

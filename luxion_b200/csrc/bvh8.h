@@ -1,0 +1,55 @@
+// bvh8.h -- compressed 8-wide BVH node shared by the host builder and the device traversal.
+//
+// The reference builds a binary binned-SAH tree with one triangle per leaf and 36-byte AoS
+// nodes (src/mesh/bvh_build.cu:15-318, include/mesh/bvh.h:10-28) and, in its active build,
+// hands the geometry to OptiX. B200 has no RT cores, so the tree here is the binned-SAH
+// binary tree collapsed into 8-wide nodes whose child boxes are quantised to 8 bits per
+// plane relative to the node's own box (the compressed wide BVH of Ylitie, Karras and Laine,
+// "Efficient Incoherent Ray Traversal on GPUs Through Compressed Wide BVHs", HPG 2017).
+//
+// Node: 80 bytes = 5 x 16 B.
+//   p[3]       f32   quantisation origin (node box minimum)
+//   e[3]       u8    per-axis scale exponent, scale = 2^(e-127)
+//   imask      u8    bit s set: slot s holds an internal child
+//   child_base u32   index of the first internal child; internal children are stored
+//                    contiguously in slot order
+//   tri_base   u32   first primitive record of the leaf slots
+//   meta[8]    u8    per slot: 0 empty; 0x80|rank internal; (count<<5)|offset leaf with
+//                    count in 1..3 primitives starting at tri_base+offset
+//   q{lo,hi}{x,y,z}[8] u8  child boxes: lo = p + q*scale (rounded outward at build time)
+// Child slots are assigned by the octant of the child centroid around the node centre, so a
+// ray visits slots in the order (slot ^ ray_octant) to go near-to-far.
+#pragma once
+#include <cstdint>
+
+namespace lux {
+
+struct alignas(16) BVH8Node {
+    float p[3];
+    uint8_t e[3];
+    uint8_t imask;
+    uint32_t child_base;
+    uint32_t tri_base;
+    uint8_t meta[8];
+    uint8_t qlox[8], qloy[8], qloz[8];
+    uint8_t qhix[8], qhiy[8], qhiz[8];
+};
+static_assert(sizeof(BVH8Node) == 80, "BVH8Node must be 80 bytes");
+
+constexpr int kMaxLeafPrims = 3;
+
+}  // namespace lux
+
+#ifndef __CUDACC__
+#include <vector>
+namespace lux {
+struct BVH8Build {
+    std::vector<BVH8Node> nodes;       // root at index 0
+    std::vector<uint32_t> prim_order;  // leaf primitive records in node order -> input prim id
+    int depth = 0;                     // BVH8 levels (root = 1)
+    double sah_cost = 0.0;
+};
+// boxes: n*6 floats (min xyz, max xyz). The builder pads nothing; callers pad boxes.
+void build_bvh8(const float* boxes, int n, BVH8Build& out);
+}  // namespace lux
+#endif

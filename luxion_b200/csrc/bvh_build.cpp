@@ -1,0 +1,321 @@
+// bvh_build.cpp -- host builder: binned-SAH binary tree collapsed into compressed 8-wide nodes.
+//
+// Binary stage: top-down, 32 bins per axis over the centroid bounds of the node, cost
+// SA(L)*nL + SA(R)*nR (the reference uses 16 bins and 1 + nL/n*SA(L) + nR/n*SA(R),
+// src/mesh/bvh_build.cu:12,167-169 -- the constant and scale do not change the argmin; its
+// 15% median fallback, :278-294, is replaced by an object-median split when binning cannot
+// separate the centroids). Leaves hold one primitive.
+// Collapse stage: each 8-wide node takes its binary node's two children and repeatedly opens
+// the child of largest surface area until 8 slots are used; subtrees of at most 3
+// primitives become leaf slots. Slots are assigned by child-centroid octant, boxes are
+// quantised outward.
+
+#include "bvh8.h"
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <deque>
+
+namespace lux {
+namespace {
+
+struct Box {
+    float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX};
+    float hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    void grow(const Box& b) {
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = std::min(lo[a], b.lo[a]);
+            hi[a] = std::max(hi[a], b.hi[a]);
+        }
+    }
+    void grow(const float* p) {
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = std::min(lo[a], p[a]);
+            hi[a] = std::max(hi[a], p[a]);
+        }
+    }
+    double area() const {
+        double d[3];
+        for (int a = 0; a < 3; ++a) d[a] = std::max(0.0, double(hi[a]) - double(lo[a]));
+        return 2.0 * (d[0] * d[1] + d[1] * d[2] + d[2] * d[0]);
+    }
+};
+
+struct BNode {
+    Box box;
+    int left = -1, right = -1;  // binary children (-1 for a leaf)
+    int begin = 0, count = 0;   // primitive range in the order array
+};
+
+struct Binary {
+    std::vector<BNode> nodes;
+    std::vector<uint32_t> order;
+};
+
+constexpr int kBins = 32;
+
+void build_binary(const float* boxes, int n, Binary& B) {
+    B.nodes.clear();
+    B.order.resize(n);
+    for (int i = 0; i < n; ++i) B.order[i] = uint32_t(i);
+    std::vector<float> cen(size_t(n) * 3);
+    for (int i = 0; i < n; ++i)
+        for (int a = 0; a < 3; ++a) cen[size_t(i) * 3 + a] = 0.5f * (boxes[i * 6 + a] + boxes[i * 6 + 3 + a]);
+    B.nodes.reserve(size_t(2 * n));
+    B.nodes.push_back(BNode());
+    B.nodes[0].begin = 0;
+    B.nodes[0].count = n;
+    std::vector<int> work{0};
+    while (!work.empty()) {
+        int ni = work.back();
+        work.pop_back();
+        BNode nd = B.nodes[ni];
+        Box cb;
+        for (int k = nd.begin; k < nd.begin + nd.count; ++k) {
+            uint32_t p = B.order[k];
+            Box pb;
+            std::memcpy(pb.lo, &boxes[size_t(p) * 6], 12);
+            std::memcpy(pb.hi, &boxes[size_t(p) * 6 + 3], 12);
+            nd.box.grow(pb);
+            cb.grow(&cen[size_t(p) * 3]);
+        }
+        if (nd.count <= 1) {
+            B.nodes[ni] = nd;
+            continue;
+        }
+        int best_axis = -1, best_split = -1;
+        double best_cost = DBL_MAX;
+        for (int a = 0; a < 3; ++a) {
+            double ext = double(cb.hi[a]) - double(cb.lo[a]);
+            if (!(ext > 0.0)) continue;
+            Box bb[kBins];
+            int bc[kBins] = {0};
+            double k1 = kBins / ext;
+            for (int k = nd.begin; k < nd.begin + nd.count; ++k) {
+                uint32_t p = B.order[k];
+                int b = int((double(cen[size_t(p) * 3 + a]) - cb.lo[a]) * k1);
+                b = std::min(kBins - 1, std::max(0, b));
+                Box pb;
+                std::memcpy(pb.lo, &boxes[size_t(p) * 6], 12);
+                std::memcpy(pb.hi, &boxes[size_t(p) * 6 + 3], 12);
+                bb[b].grow(pb);
+                bc[b]++;
+            }
+            double ra[kBins];
+            int rc[kBins];
+            Box acc;
+            int cnt = 0;
+            for (int b = kBins - 1; b > 0; --b) {
+                acc.grow(bb[b]);
+                cnt += bc[b];
+                ra[b] = acc.area();
+                rc[b] = cnt;
+            }
+            Box lacc;
+            int lcnt = 0;
+            for (int b = 0; b < kBins - 1; ++b) {
+                lacc.grow(bb[b]);
+                lcnt += bc[b];
+                if (lcnt == 0 || rc[b + 1] == 0) continue;
+                double c = lacc.area() * lcnt + ra[b + 1] * rc[b + 1];
+                if (c < best_cost) {
+                    best_cost = c;
+                    best_axis = a;
+                    best_split = b;
+                }
+            }
+        }
+        int mid;
+        if (best_axis >= 0) {
+            int a = best_axis;
+            double ext = double(cb.hi[a]) - double(cb.lo[a]);
+            double k1 = kBins / ext;
+            auto it = std::partition(B.order.begin() + nd.begin, B.order.begin() + nd.begin + nd.count, [&](uint32_t p) {
+                int b = int((double(cen[size_t(p) * 3 + a]) - cb.lo[a]) * k1);
+                b = std::min(kBins - 1, std::max(0, b));
+                return b <= best_split;
+            });
+            mid = int(it - B.order.begin());
+        } else {
+            mid = nd.begin + nd.count / 2;  // coincident centroids: split the range in half
+        }
+        if (mid <= nd.begin || mid >= nd.begin + nd.count) mid = nd.begin + nd.count / 2;
+        int l = int(B.nodes.size());
+        B.nodes.push_back(BNode());
+        B.nodes.push_back(BNode());
+        nd.left = l;
+        nd.right = l + 1;
+        B.nodes[l].begin = nd.begin;
+        B.nodes[l].count = mid - nd.begin;
+        B.nodes[l + 1].begin = mid;
+        B.nodes[l + 1].count = nd.begin + nd.count - mid;
+        B.nodes[ni] = nd;
+        work.push_back(l);
+        work.push_back(l + 1);
+    }
+}
+
+// Quantise the child boxes of one 8-wide node. The node box is first widened by a relative
+// 1e-5 of its largest extent (plus 1e-7 of its coordinate magnitude) and every child plane
+// is rounded outward by a further 1% of a quantisation step, which dominates the rounding
+// error of the device slab test (a few ulps of the node extent).
+void encode_node(BVH8Node& N, const Box& nb, const Box* cbox, const bool* used) {
+    double mext = 0.0, mabs = 0.0;
+    for (int a = 0; a < 3; ++a) {
+        mext = std::max(mext, double(nb.hi[a]) - double(nb.lo[a]));
+        mabs = std::max(mabs, std::max(std::fabs(double(nb.lo[a])), std::fabs(double(nb.hi[a]))));
+    }
+    const double pad = 1e-5 * mext + 1e-7 * mabs + 1e-30;
+    double hi_d[3];
+    for (int a = 0; a < 3; ++a) {
+        double lo_d = double(nb.lo[a]) - pad;
+        hi_d[a] = double(nb.hi[a]) + pad;
+        float pf = float(lo_d);
+        if (double(pf) > lo_d) pf = std::nextafter(pf, -FLT_MAX);
+        N.p[a] = pf;
+    }
+    for (int a = 0; a < 3; ++a) {
+        double ext = hi_d[a] - double(N.p[a]);
+        int e = -126;
+        if (ext > 0.0) e = int(std::ceil(std::log2(ext / 255.0)));
+        e = std::max(-126, std::min(127, e));
+        // make sure 255 steps cover the extent after the exponent rounding
+        while (std::ldexp(255.0, e) < ext && e < 127) ++e;
+        N.e[a] = uint8_t(e + 127);
+    }
+    uint8_t* qlo[3] = {N.qlox, N.qloy, N.qloz};
+    uint8_t* qhi[3] = {N.qhix, N.qhiy, N.qhiz};
+    for (int s = 0; s < 8; ++s) {
+        for (int a = 0; a < 3; ++a) {
+            if (!used[s]) {
+                qlo[a][s] = 0xff;
+                qhi[a][s] = 0x00;
+                continue;
+            }
+            double scale = std::ldexp(1.0, int(N.e[a]) - 127);
+            double lo = std::floor((double(cbox[s].lo[a]) - double(N.p[a])) / scale - 0.01);
+            double hi = std::ceil((double(cbox[s].hi[a]) - double(N.p[a])) / scale + 0.01);
+            qlo[a][s] = uint8_t(std::max(0.0, std::min(255.0, lo)));
+            qhi[a][s] = uint8_t(std::max(0.0, std::min(255.0, hi)));
+        }
+    }
+}
+
+}  // namespace
+
+void build_bvh8(const float* boxes, int n, BVH8Build& out) {
+    out.nodes.clear();
+    out.prim_order.clear();
+    out.depth = 0;
+    out.sah_cost = 0.0;
+    if (n <= 0) return;
+    Binary B;
+    build_binary(boxes, n, B);
+    struct Item {
+        int bnode;
+        int out_index;
+        int level;
+    };
+    std::deque<Item> q;
+    out.nodes.push_back(BVH8Node());
+    q.push_back({0, 0, 1});
+    const double root_area = std::max(1e-30, B.nodes[0].box.area());
+    while (!q.empty()) {
+        Item it = q.front();
+        q.pop_front();
+        out.depth = std::max(out.depth, it.level);
+        const BNode& bn = B.nodes[it.bnode];
+        // gather up to 8 children
+        std::vector<int> ch;
+        if (bn.left < 0 || bn.count <= kMaxLeafPrims) {
+            ch.push_back(it.bnode);  // the whole node is one leaf slot
+        } else {
+            ch.push_back(bn.left);
+            ch.push_back(bn.right);
+            while (ch.size() < 8) {
+                int pick = -1;
+                double pa = -1.0;
+                for (size_t k = 0; k < ch.size(); ++k) {
+                    const BNode& c = B.nodes[ch[k]];
+                    if (c.left < 0 || c.count <= kMaxLeafPrims) continue;
+                    double a = c.box.area();
+                    if (a > pa) {
+                        pa = a;
+                        pick = int(k);
+                    }
+                }
+                if (pick < 0) break;
+                int c = ch[pick];
+                ch[pick] = B.nodes[c].left;
+                ch.push_back(B.nodes[c].right);
+            }
+        }
+        // slot assignment by centroid octant around the node centre
+        float ctr[3];
+        for (int a = 0; a < 3; ++a) ctr[a] = 0.5f * (bn.box.lo[a] + bn.box.hi[a]);
+        int slot_of[8];
+        bool slot_used[8] = {false};
+        {
+            struct P {
+                double cost;
+                int c, s;
+            };
+            std::vector<P> ps;
+            for (size_t k = 0; k < ch.size(); ++k) {
+                const Box& b = B.nodes[ch[k]].box;
+                double d[3];
+                for (int a = 0; a < 3; ++a) d[a] = 0.5 * (double(b.lo[a]) + double(b.hi[a])) - ctr[a];
+                for (int s = 0; s < 8; ++s) {
+                    double c = 0;
+                    for (int a = 0; a < 3; ++a) c += ((s >> a) & 1) ? -d[a] : d[a];
+                    ps.push_back({c, int(k), s});
+                }
+            }
+            std::sort(ps.begin(), ps.end(), [](const P& x, const P& y) {
+                return x.cost < y.cost || (x.cost == y.cost && (x.c < y.c || (x.c == y.c && x.s < y.s)));
+            });
+            bool cdone[8] = {false};
+            for (const P& p : ps) {
+                if (cdone[p.c] || slot_used[p.s]) continue;
+                cdone[p.c] = true;
+                slot_used[p.s] = true;
+                slot_of[p.c] = p.s;
+            }
+        }
+        BVH8Node N;
+        std::memset(&N, 0, sizeof(N));
+        Box cbox[8];
+        int child_at_slot[8];
+        for (int s = 0; s < 8; ++s) child_at_slot[s] = -1;
+        for (size_t k = 0; k < ch.size(); ++k) {
+            child_at_slot[slot_of[k]] = ch[k];
+            cbox[slot_of[k]] = B.nodes[ch[k]].box;
+        }
+        encode_node(N, bn.box, cbox, slot_used);
+        N.child_base = uint32_t(out.nodes.size());
+        N.tri_base = uint32_t(out.prim_order.size());
+        int rank = 0;
+        for (int s = 0; s < 8; ++s) {
+            int c = child_at_slot[s];
+            if (c < 0) continue;
+            const BNode& cn = B.nodes[c];
+            out.sah_cost += cn.box.area() / root_area;
+            if (cn.left < 0 || cn.count <= kMaxLeafPrims) {
+                int off = int(out.prim_order.size()) - int(N.tri_base);
+                for (int k = cn.begin; k < cn.begin + cn.count; ++k) out.prim_order.push_back(B.order[k]);
+                N.meta[s] = uint8_t((cn.count << 5) | off);
+            } else {
+                N.imask |= uint8_t(1u << s);
+                N.meta[s] = uint8_t(0x80 | rank);
+                out.nodes.push_back(BVH8Node());
+                q.push_back({c, int(out.nodes.size()) - 1, it.level + 1});
+                ++rank;
+            }
+        }
+        out.nodes[it.out_index] = N;
+    }
+}
+
+}  // namespace lux

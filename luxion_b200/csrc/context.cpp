@@ -1,0 +1,1150 @@
+// context.cpp -- host side of the C-ABI (include/luxion.h): scene upload, acceleration
+// structure build, light tables, wavefront buffers and the device-side bounce loop.
+//
+// Reference mapping:
+//   lux_init         pathtraceInit (src/pathtrace/pathtrace_buffers.cu:21-140) together with
+//                    the per-mesh uploads and acceleration builds main() does before it
+//                    (src/main.cpp:199-274) and the scene precompute
+//                    (src/scene/scene_precompute.cpp:22-124)
+//   lux_render_iter  pathtrace (src/pathtrace.cu:97-367): one sample per pixel
+//   lux_render       the same loop, several samples in flight per wave
+//   lux_free         pathtraceFree (src/pathtrace/pathtrace_buffers.cu:142-177)
+//   lux_copy_image   copyImageToHost (src/pathtrace/pathtrace_buffers.cu:180-190)
+// Unlike the reference, no step of a bounce returns to the host: queue lengths live in
+// device counters that the kernels read, so a whole wave is one stream of launches that can
+// be captured once as a CUDA graph and replayed.
+
+#include "../../include/luxion.h"
+#include "bvh8.h"
+#include "device_scene.h"
+#include "launch.h"
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <thread>
+#include <vector>
+
+using namespace lux;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define LUX_CUDA(call)                                                                      \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess) {                                                            \
+            return fail(e_ == cudaErrorMemoryAllocation ? LUX_ERR_OOM : LUX_ERR_CUDA,       \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                \
+        }                                                                                   \
+    } while (0)
+
+template <class T>
+int dalloc(T** p, size_t n) {
+    *p = nullptr;
+    if (n == 0) return LUX_OK;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(T));
+    if (e != cudaSuccess) return fail(LUX_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    return LUX_OK;
+}
+template <class T>
+int upload(T** p, const T* src, size_t n) {
+    int rc = dalloc(p, n);
+    if (rc) return rc;
+    if (n) LUX_CUDA(cudaMemcpy(*p, src, n * sizeof(T), cudaMemcpyHostToDevice));
+    return LUX_OK;
+}
+
+struct DevTex {
+    cudaArray_t arr = nullptr;
+    cudaTextureObject_t obj = 0;
+    size_t bytes = 0;
+};
+
+bool invert4(const float* m, double* out) {
+    double t[4][8];
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) {
+            t[r][c] = m[c * 4 + r];
+            t[r][c + 4] = (r == c) ? 1.0 : 0.0;
+        }
+    for (int c = 0; c < 4; ++c) {
+        int p = c;
+        for (int r = c + 1; r < 4; ++r)
+            if (std::fabs(t[r][c]) > std::fabs(t[p][c])) p = r;
+        if (std::fabs(t[p][c]) < 1e-300) return false;
+        for (int k = 0; k < 8; ++k) std::swap(t[c][k], t[p][k]);
+        double d = t[c][c];
+        for (int k = 0; k < 8; ++k) t[c][k] /= d;
+        for (int r = 0; r < 4; ++r)
+            if (r != c) {
+                double f = t[r][c];
+                for (int k = 0; k < 8; ++k) t[r][k] -= f * t[c][k];
+            }
+    }
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) out[c * 4 + r] = t[r][c + 4];
+    return true;
+}
+
+}  // namespace
+
+struct lux_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    lux_options opt{};
+    DevOptions dopt{};
+    DevCamera cam{};
+    DevScene S{};
+    DevWave W{};
+    int width = 0, height = 0, npix = 0;
+    int spp_per_wave = 1;
+    int accumulated = 0;
+    // owned device memory
+    std::vector<void*> allocs;
+    std::vector<DevTex> texs;
+    DevTex env;
+    float* image = nullptr;
+    float* comp = nullptr;
+    uint8_t* rgba = nullptr;
+    void* sort_temp = nullptr;
+    size_t sort_temp_bytes = 0;
+    int* h_wave_iter = nullptr;          // pinned, two ints per wave of the current call
+    WaveCounters* h_ctr = nullptr;       // pinned, one per wave of the current call
+    int h_cap = 0;
+    // graphs per wave size
+    std::map<int, cudaGraphExec_t> graphs;
+    // stats of the last call
+    lux_stats stats{};
+    bool timing = false;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    std::vector<cudaEvent_t> kev;
+    // host copies for CDF queries
+    std::vector<float> h_emissive_prefix, h_tri_prefix, h_marginal, h_conditional;
+    float h_total_area = 0.0f;
+    int64_t instanced_tris = 0;
+    size_t scene_bytes = 0;
+
+    template <class T>
+    int alloc(T** p, size_t n) {
+        int rc = dalloc(p, n);
+        if (rc == LUX_OK && *p) allocs.push_back(*p);
+        return rc;
+    }
+    template <class T>
+    int up(T** p, const T* src, size_t n) {
+        int rc = upload(p, src, n);
+        if (rc == LUX_OK && *p) allocs.push_back(*p);
+        scene_bytes += n * sizeof(T);
+        return rc;
+    }
+};
+
+namespace {
+
+float half_bits_to_float(uint16_t h) {
+    __half_raw r;
+    r.x = h;
+    return __half2float(__half(r));
+}
+
+// Upload one texture. storage LUX_TEXSTORE_FLOAT converts 8/16-bit unorm texels to float4 as
+// TextureHandler::load_textures_on_device does (c/255, c/65535; src/texture.cu:12-69),
+// LUX_TEXSTORE_HALF converts them to binary16, LUX_TEXSTORE_UNORM8 keeps 8-bit texels.
+int make_texture(const lux_texture_desc& t, DevTex& out, int storage) {
+    if (t.width <= 0 || t.height <= 0 || !t.data) return fail(LUX_ERR_INVALID, "empty texture");
+    const size_t n = size_t(t.width) * t.height * 4;
+    std::vector<float> f32;
+    std::vector<__half> f16;
+    const void* src = t.data;
+    int fmt = t.format;
+    auto to_float = [&](size_t i) -> float {
+        switch (t.format) {
+            case LUX_TEX_RGBA8: return float(static_cast<const uint8_t*>(t.data)[i]) / 255.0f;
+            case LUX_TEX_RGBA16: return float(static_cast<const uint16_t*>(t.data)[i]) / 65535.0f;
+            case LUX_TEX_RGBA16F: return half_bits_to_float(static_cast<const uint16_t*>(t.data)[i]);
+            default: return static_cast<const float*>(t.data)[i];
+        }
+    };
+    if (storage == LUX_TEXSTORE_HALF && t.format != LUX_TEX_RGBA16F) {
+        f16.resize(n);
+        for (size_t i = 0; i < n; ++i) f16[i] = __float2half_rn(to_float(i));
+        src = f16.data();
+        fmt = LUX_TEX_RGBA16F;
+    } else if (storage == LUX_TEXSTORE_FLOAT && (t.format == LUX_TEX_RGBA8 || t.format == LUX_TEX_RGBA16)) {
+        f32.resize(n);
+        for (size_t i = 0; i < n; ++i) f32[i] = to_float(i);
+        src = f32.data();
+        fmt = LUX_TEX_RGBA32F;
+    }
+    cudaChannelFormatDesc fd;
+    size_t texel;
+    cudaTextureReadMode rm = cudaReadModeElementType;
+    switch (fmt) {
+        case LUX_TEX_RGBA8:
+            fd = cudaCreateChannelDesc<uchar4>();
+            texel = 4;
+            rm = cudaReadModeNormalizedFloat;
+            break;
+        case LUX_TEX_RGBA16:
+            fd = cudaCreateChannelDesc<ushort4>();
+            texel = 8;
+            rm = cudaReadModeNormalizedFloat;
+            break;
+        case LUX_TEX_RGBA16F:
+            fd = cudaCreateChannelDescHalf4();
+            texel = 8;
+            break;
+        case LUX_TEX_RGBA32F:
+            fd = cudaCreateChannelDesc<float4>();
+            texel = 16;
+            break;
+        default:
+            return fail(LUX_ERR_INVALID, "unknown texture format");
+    }
+    LUX_CUDA(cudaMallocArray(&out.arr, &fd, t.width, t.height));
+    LUX_CUDA(cudaMemcpy2DToArray(out.arr, 0, 0, src, size_t(t.width) * texel, size_t(t.width) * texel, t.height,
+                                 cudaMemcpyHostToDevice));
+    out.bytes = size_t(t.width) * t.height * texel;
+    cudaResourceDesc rd{};
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = out.arr;
+    cudaTextureDesc td{};
+    td.addressMode[0] = cudaAddressModeWrap;
+    td.addressMode[1] = cudaAddressModeWrap;
+    td.filterMode = cudaFilterModeLinear;
+    td.readMode = rm;
+    td.normalizedCoords = 1;
+    LUX_CUDA(cudaCreateTextureObject(&out.obj, &rd, &td, nullptr));
+    return LUX_OK;
+}
+
+// Texel values as the reference holds them (float4) for the HDRI CDF build.
+void env_texels(const lux_scene_desc& d, std::vector<float>& out) {
+    size_t n = size_t(d.env_width) * d.env_height * 4;
+    out.resize(n);
+    if (d.env_format == LUX_TEX_RGBA16F) {
+        const uint16_t* s = static_cast<const uint16_t*>(d.env_data);
+        for (size_t i = 0; i < n; ++i) out[i] = half_bits_to_float(s[i]);
+    } else {
+        const float* s = static_cast<const float*>(d.env_data);
+        std::copy(s, s + n, out.begin());
+    }
+}
+
+// Emissive-area and HDRI CDFs as Scene::precompute_emissive_mesh_area and
+// precompute_hdri_emission build them (src/scene/scene_precompute.cpp:22-124): sequential
+// prefix sums in T, then normalised. T = float reproduces the reference bit for bit; the
+// precision form uses T = double and rounds the final tables to float.
+template <class T>
+bool light_tables(const lux_scene_desc& d, const std::vector<float>& env, std::vector<int>& emissive,
+                  std::vector<float>& eprefix, std::vector<std::vector<float>>& tri_prefix, float& total_area,
+                  std::vector<float>& marginal, std::vector<float>& conditional) {
+    const float kEPS = 0.00001f;
+    T area = T(0);
+    std::vector<T> ep;
+    emissive.clear();
+    tri_prefix.assign(d.num_instances, {});
+    for (int i = 0; i < d.num_instances; ++i) {
+        const lux_instance_desc& in = d.instances[i];
+        const lux_mesh_desc& m = d.meshes[in.mesh];
+        const lux_material_desc& mat = d.materials[in.material];
+        float ec = std::sqrt(mat.emission_color[0] * mat.emission_color[0] + mat.emission_color[1] * mat.emission_color[1] +
+                             mat.emission_color[2] * mat.emission_color[2]);
+        bool is_em = ec * mat.emission_strength > kEPS;
+        if (!is_em) continue;  // only emissive instances' triangle tables are ever read
+        T cum = T(0);
+        std::vector<T> tp(m.num_tris);
+        for (int k = 0; k < m.num_tris; ++k) {
+            T P[3][3];
+            for (int c = 0; c < 3; ++c) {
+                const float* v = m.positions + size_t(m.indices[k * 3 + c]) * 3;
+                for (int r = 0; r < 3; ++r) {
+                    T a0 = T(in.transform[0 * 4 + r]) * T(v[0]), a1 = T(in.transform[1 * 4 + r]) * T(v[1]);
+                    T a2 = T(in.transform[2 * 4 + r]) * T(v[2]), a3 = T(in.transform[3 * 4 + r]) * T(1);
+                    P[c][r] = (a0 + a1) + (a2 + a3);
+                }
+            }
+            T u[3], v[3];
+            for (int r = 0; r < 3; ++r) {
+                u[r] = P[1][r] - P[0][r];
+                v[r] = P[2][r] - P[0][r];
+            }
+            T cx = u[1] * v[2] - v[1] * u[2], cy = u[2] * v[0] - v[2] * u[0], cz = u[0] * v[1] - v[0] * u[1];
+            cum += T(0.5) * std::sqrt(cx * cx + cy * cy + cz * cz);
+            tp[k] = cum;
+        }
+        tri_prefix[i].resize(m.num_tris);
+        for (int k = 0; k < m.num_tris; ++k) tri_prefix[i][k] = float(tp[k] / cum);
+        area += cum;
+        emissive.push_back(i);
+        ep.push_back(area);
+    }
+    eprefix.resize(ep.size());
+    for (size_t k = 0; k < ep.size(); ++k) eprefix[k] = float(ep[k] / area);
+    total_area = float(area);
+    marginal.clear();
+    conditional.clear();
+    if (!d.env_data) return true;
+    const int W = d.env_width, H = d.env_height;
+    const float kPI = 3.1415926535897932384626422832795028841971f;
+    std::vector<T> cond(size_t(W) * H), marg(H);
+    T total = T(0);
+    for (int y = 0; y < H; ++y) {
+        T rt = T(0);
+        T theta = T(kPI) * (T(y) + T(0.5f)) / T(H);
+        T st = std::sin(theta);
+        for (int x = 0; x < W; ++x) {
+            const float* p = &env[(size_t(y) * W + x) * 4];
+            T a = T(p[0]) * T(p[0]), b = T(p[1]) * T(p[1]), c = T(p[2]) * T(p[2]), dd = T(p[3]) * T(p[3]);
+            T e = std::sqrt((a + b) + (c + dd));
+            rt += e * st;
+            cond[size_t(y) * W + x] = rt;
+        }
+        if (rt > T(0)) {
+            for (int x = 0; x < W; ++x) cond[size_t(y) * W + x] /= rt;
+        } else {
+            for (int x = 0; x < W; ++x) cond[size_t(y) * W + x] = T(x + 1) / T(W);
+        }
+        cond[size_t(y) * W + (W - 1)] = T(1);
+        total += rt;
+        marg[y] = total;
+    }
+    if (total == T(0)) return false;  // the reference exits: "HDRI has emission of 0.0f"
+    for (int y = 0; y < H; ++y) marg[y] /= total;
+    marg[H - 1] = T(1);
+    marginal.resize(H);
+    conditional.resize(size_t(W) * H);
+    for (int y = 0; y < H; ++y) marginal[y] = float(marg[y]);
+    for (size_t k = 0; k < cond.size(); ++k) conditional[k] = float(cond[k]);
+    return true;
+}
+
+int build_scene(lux_ctx* C, const lux_scene_desc& d) {
+    // ---- per-mesh BLAS (threaded across meshes) ----
+    const int NM = d.num_meshes;
+    std::vector<BVH8Build> blas(NM);
+    {
+        std::atomic<int> next{0};
+        unsigned nt = std::max(1u, std::min(std::thread::hardware_concurrency(), 64u));
+        auto work = [&]() {
+            for (int m = next++; m < NM; m = next++) {
+                const lux_mesh_desc& md = d.meshes[m];
+                std::vector<float> boxes(size_t(md.num_tris) * 6);
+                for (int k = 0; k < md.num_tris; ++k) {
+                    float* b = &boxes[size_t(k) * 6];
+                    for (int a = 0; a < 3; ++a) {
+                        b[a] = FLT_MAX;
+                        b[3 + a] = -FLT_MAX;
+                    }
+                    for (int c = 0; c < 3; ++c) {
+                        const float* v = md.positions + size_t(md.indices[k * 3 + c]) * 3;
+                        for (int a = 0; a < 3; ++a) {
+                            b[a] = std::min(b[a], v[a]);
+                            b[3 + a] = std::max(b[3 + a], v[a]);
+                        }
+                    }
+                    for (int a = 0; a < 3; ++a) {
+                        float pad = 1e-6f * std::max(std::fabs(b[a]), std::fabs(b[3 + a])) + 1e-9f;
+                        b[a] -= pad;
+                        b[3 + a] += pad;
+                    }
+                }
+                build_bvh8(boxes.data(), md.num_tris, blas[m]);
+            }
+        };
+        std::vector<std::thread> th;
+        for (unsigned t = 0; t + 1 < nt; ++t) th.emplace_back(work);
+        work();
+        for (auto& t : th) t.join();
+    }
+    // ---- concatenate meshes ----
+    std::vector<BVH8Node> nodes;
+    std::vector<float4> prims;
+    std::vector<float> pos, nrm, uv;
+    std::vector<uint32_t> idx;
+    std::vector<uint32_t> mesh_root(NM), mesh_prim(NM), mesh_vert(NM), mesh_idx(NM);
+    std::vector<int> mesh_flags(NM);
+    std::vector<float> mesh_box(size_t(NM) * 6);
+    bool any_n = false, any_uv = false;
+    for (int m = 0; m < NM; ++m) {
+        any_n |= d.meshes[m].normals != nullptr;
+        any_uv |= d.meshes[m].uvs != nullptr;
+    }
+    int max_blas_depth = 0;
+    for (int m = 0; m < NM; ++m) {
+        const lux_mesh_desc& md = d.meshes[m];
+        const BVH8Build& B = blas[m];
+        max_blas_depth = std::max(max_blas_depth, B.depth);
+        uint32_t nb = uint32_t(nodes.size());
+        mesh_root[m] = nb;
+        for (BVH8Node n : B.nodes) {
+            n.child_base += nb;
+            nodes.push_back(n);
+        }
+        mesh_prim[m] = uint32_t(prims.size() / 3);
+        for (uint32_t p : B.prim_order) {
+            const float* v0 = md.positions + size_t(md.indices[p * 3]) * 3;
+            const float* v1 = md.positions + size_t(md.indices[p * 3 + 1]) * 3;
+            const float* v2 = md.positions + size_t(md.indices[p * 3 + 2]) * 3;
+            float pf;
+            int32_t pi = int32_t(p);
+            std::memcpy(&pf, &pi, 4);
+            prims.push_back(make_float4(v0[0], v0[1], v0[2], pf));
+            prims.push_back(make_float4(v1[0] - v0[0], v1[1] - v0[1], v1[2] - v0[2], 0.0f));
+            prims.push_back(make_float4(v2[0] - v0[0], v2[1] - v0[1], v2[2] - v0[2], 0.0f));
+        }
+        mesh_vert[m] = uint32_t(pos.size() / 3);
+        mesh_idx[m] = uint32_t(idx.size() / 3);
+        pos.insert(pos.end(), md.positions, md.positions + size_t(md.num_verts) * 3);
+        if (any_n) {
+            if (md.normals) nrm.insert(nrm.end(), md.normals, md.normals + size_t(md.num_verts) * 3);
+            else nrm.insert(nrm.end(), size_t(md.num_verts) * 3, 0.0f);
+        }
+        if (any_uv) {
+            if (md.uvs) uv.insert(uv.end(), md.uvs, md.uvs + size_t(md.num_verts) * 2);
+            else uv.insert(uv.end(), size_t(md.num_verts) * 2, 0.0f);
+        }
+        idx.insert(idx.end(), md.indices, md.indices + size_t(md.num_tris) * 3);
+        mesh_flags[m] = (md.normals ? kInstHasNormals : 0) | (md.uvs ? kInstHasUVs : 0);
+        float* b = &mesh_box[size_t(m) * 6];
+        for (int a = 0; a < 3; ++a) {
+            b[a] = FLT_MAX;
+            b[3 + a] = -FLT_MAX;
+        }
+        for (int v = 0; v < md.num_verts; ++v)
+            for (int a = 0; a < 3; ++a) {
+                b[a] = std::min(b[a], md.positions[size_t(v) * 3 + a]);
+                b[3 + a] = std::max(b[3 + a], md.positions[size_t(v) * 3 + a]);
+            }
+    }
+    // ---- instances + TLAS ----
+    const int NI = d.num_instances;
+    std::vector<DevInstance> insts(NI);
+    std::vector<float> iboxes(size_t(NI) * 6);
+    C->instanced_tris = 0;
+    for (int i = 0; i < NI; ++i) {
+        const lux_instance_desc& in = d.instances[i];
+        DevInstance& I = insts[i];
+        float inv[16], invT[16];
+        if (in.has_inverse) {
+            std::memcpy(inv, in.inverse, 64);
+            std::memcpy(invT, in.inv_transpose, 64);
+        } else {
+            double id[16];
+            if (!invert4(in.transform, id)) return fail(LUX_ERR_INVALID, "singular instance transform");
+            for (int k = 0; k < 16; ++k) inv[k] = float(id[k]);
+            for (int c = 0; c < 4; ++c)
+                for (int r = 0; r < 4; ++r) invT[c * 4 + r] = float(id[r * 4 + c]);
+        }
+        for (int c = 0; c < 4; ++c)
+            for (int r = 0; r < 3; ++r) {
+                I.M[c * 3 + r] = in.transform[c * 4 + r];
+                I.Minv[c * 3 + r] = inv[c * 4 + r];
+                I.MinvT[c * 3 + r] = invT[c * 4 + r];
+            }
+        I.mesh = in.mesh;
+        I.material = in.material;
+        I.blas_root = mesh_root[in.mesh];
+        I.prim_base = mesh_prim[in.mesh];
+        I.vert_base = mesh_vert[in.mesh];
+        I.idx_base = mesh_idx[in.mesh];
+        const lux_material_desc& mat = d.materials[in.material];
+        I.flags = mesh_flags[in.mesh] | (mat.alpha_mode != LUX_ALPHA_OPAQUE ? kInstAnyHit : 0);
+        I.num_tris = d.meshes[in.mesh].num_tris;
+        C->instanced_tris += I.num_tris;
+        // world box: 8 transformed corners of the mesh box, in double, padded
+        const float* mb = &mesh_box[size_t(in.mesh) * 6];
+        float* b = &iboxes[size_t(i) * 6];
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+        for (int c = 0; c < 8; ++c) {
+            double p[3] = {(c & 1) ? mb[3] : mb[0], (c & 2) ? mb[4] : mb[1], (c & 4) ? mb[5] : mb[2]};
+            for (int a = 0; a < 3; ++a) {
+                double w = double(in.transform[0 * 4 + a]) * p[0] + double(in.transform[1 * 4 + a]) * p[1] +
+                           double(in.transform[2 * 4 + a]) * p[2] + double(in.transform[3 * 4 + a]);
+                lo[a] = std::min(lo[a], w);
+                hi[a] = std::max(hi[a], w);
+            }
+        }
+        double mext = 0, mabs = 0;
+        for (int a = 0; a < 3; ++a) {
+            mext = std::max(mext, hi[a] - lo[a]);
+            mabs = std::max(mabs, std::max(std::fabs(lo[a]), std::fabs(hi[a])));
+        }
+        double pad = 1e-5 * mext + 1e-6 * mabs + 1e-12;
+        for (int a = 0; a < 3; ++a) {
+            b[a] = float(lo[a] - pad);
+            b[3 + a] = float(hi[a] + pad);
+        }
+    }
+    BVH8Build tl;
+    build_bvh8(iboxes.data(), NI, tl);
+    uint32_t tlas_root = uint32_t(nodes.size());
+    for (BVH8Node n : tl.nodes) {
+        n.child_base += tlas_root;
+        nodes.push_back(n);
+    }
+    std::vector<uint32_t> tlas_prims(tl.prim_order.begin(), tl.prim_order.end());
+    if (tl.depth + max_blas_depth + 4 > 16 + 48)
+        return fail(LUX_ERR_UNSUPPORTED, "acceleration structure deeper than the traversal stack");
+    // ---- materials + textures ----
+    C->texs.resize(d.num_textures);
+    for (int t = 0; t < d.num_textures; ++t) {
+        int rc = make_texture(d.textures[t], C->texs[t], C->opt.texture_storage);
+        if (rc) return rc;
+    }
+    std::vector<DevMaterial> mats(d.num_materials);
+    for (int k = 0; k < d.num_materials; ++k) {
+        const lux_material_desc& s = d.materials[k];
+        DevMaterial& m = mats[k];
+        std::memset(&m, 0, sizeof(m));
+        for (int c = 0; c < 3; ++c) {
+            m.color[c] = s.color[c];
+            m.emission[c] = s.emission_color[c] * s.emission_strength;
+        }
+        m.alpha = s.alpha;
+        m.roughness = s.roughness;
+        m.metallic = s.metallic;
+        m.transmission = s.transmission;
+        m.ior = s.ior;
+        m.alpha_cutoff = s.alpha_cutoff;
+        m.alpha_mode = s.alpha_mode;
+        auto tex_of = [&](int t, int flag, unsigned long long& obj) -> int {
+            if (t < 0) return LUX_OK;
+            if (t >= d.num_textures) return fail(LUX_ERR_INVALID, "material texture index out of range");
+            obj = C->texs[t].obj;
+            m.flags |= flag;
+            return LUX_OK;
+        };
+        int rc = tex_of(s.albedo_tex, kMatAlbedoTex, m.albedo_tex);
+        rc = rc ? rc : tex_of(s.emissive_tex, kMatEmissiveTex, m.emissive_tex);
+        rc = rc ? rc : tex_of(s.normal_tex, kMatNormalTex, m.normal_tex);
+        rc = rc ? rc : tex_of(s.metallic_roughness_tex, kMatMRTex, m.mr_tex);
+        if (rc) return rc;
+        auto tt = [](const lux_tex_transform& a, DevTexTransform& b) {
+            b.offset[0] = a.offset[0];
+            b.offset[1] = a.offset[1];
+            b.scale[0] = a.scale[0];
+            b.scale[1] = a.scale[1];
+            b.rotation = a.rotation;
+        };
+        tt(s.albedo_tt, m.albedo_tt);
+        tt(s.emissive_tt, m.emissive_tt);
+        tt(s.normal_tt, m.normal_tt);
+        tt(s.metallic_roughness_tt, m.mr_tt);
+    }
+    // ---- light tables ----
+    std::vector<float> envt;
+    if (d.env_data) env_texels(d, envt);
+    std::vector<int> emissive;
+    std::vector<std::vector<float>> tri_prefix;
+    bool env_ok;
+    if (C->opt.precision == LUX_PRECISION_COMPENSATED)
+        env_ok = light_tables<double>(d, envt, emissive, C->h_emissive_prefix, tri_prefix, C->h_total_area,
+                                      C->h_marginal, C->h_conditional);
+    else
+        env_ok = light_tables<float>(d, envt, emissive, C->h_emissive_prefix, tri_prefix, C->h_total_area,
+                                     C->h_marginal, C->h_conditional);
+    if (!env_ok) return fail(LUX_ERR_INVALID, "environment map has no emission");
+    std::vector<int> tri_off;
+    C->h_tri_prefix.clear();
+    for (int e : emissive) {
+        tri_off.push_back(int(C->h_tri_prefix.size()));
+        C->h_tri_prefix.insert(C->h_tri_prefix.end(), tri_prefix[e].begin(), tri_prefix[e].end());
+    }
+    if (C->opt.direct_light_sampling && (emissive.empty() || C->h_total_area < 0.00001f))
+        return fail(LUX_ERR_INVALID, "-dmis requires the scene to contain emissive geometry");
+    if (C->opt.env_importance_sampling && !d.env_data)
+        return fail(LUX_ERR_INVALID, "-emis requires an environment map");
+    if (d.env_data) {
+        lux_texture_desc et{d.env_width, d.env_height, d.env_format, 0, d.env_data};
+        int rc = make_texture(et, C->env, C->opt.texture_storage == LUX_TEXSTORE_HALF ? LUX_TEXSTORE_HALF : LUX_TEXSTORE_FLOAT);
+        if (rc) return rc;
+    }
+    // ---- upload ----
+    DevScene& S = C->S;
+    std::memset(&S, 0, sizeof(S));
+    uint4* dn = nullptr;
+    int rc = C->up(&dn, reinterpret_cast<const uint4*>(nodes.data()), nodes.size() * 5);
+    if (rc) return rc;
+    S.nodes = dn;
+    float4* dp = nullptr;
+    if ((rc = C->up(&dp, prims.data(), prims.size()))) return rc;
+    S.prims = dp;
+    DevInstance* di = nullptr;
+    if ((rc = C->up(&di, insts.data(), insts.size()))) return rc;
+    S.insts = di;
+    uint32_t* dt = nullptr;
+    if ((rc = C->up(&dt, tlas_prims.data(), tlas_prims.size()))) return rc;
+    S.tlas_prims = dt;
+    S.tlas_root = tlas_root;
+    S.num_insts = NI;
+    float* f = nullptr;
+    if ((rc = C->up(&f, pos.data(), pos.size()))) return rc;
+    S.pos = f;
+    if (any_n) {
+        if ((rc = C->up(&f, nrm.data(), nrm.size()))) return rc;
+        S.nrm = f;
+    }
+    if (any_uv) {
+        if ((rc = C->up(&f, uv.data(), uv.size()))) return rc;
+        S.uv = f;
+    }
+    uint32_t* du = nullptr;
+    if ((rc = C->up(&du, idx.data(), idx.size()))) return rc;
+    S.idx = du;
+    DevMaterial* dm = nullptr;
+    if ((rc = C->up(&dm, mats.data(), mats.size()))) return rc;
+    S.mats = dm;
+    int* ei = nullptr;
+    if ((rc = C->up(&ei, emissive.data(), emissive.size()))) return rc;
+    S.emissive_inst = ei;
+    if ((rc = C->up(&f, C->h_emissive_prefix.data(), C->h_emissive_prefix.size()))) return rc;
+    S.emissive_prefix = f;
+    if ((rc = C->up(&f, C->h_tri_prefix.data(), C->h_tri_prefix.size()))) return rc;
+    S.tri_prefix = f;
+    if ((rc = C->up(&ei, tri_off.data(), tri_off.size()))) return rc;
+    S.tri_prefix_off = ei;
+    S.num_emissive = int(emissive.size());
+    S.total_area = C->h_total_area;
+    if (d.env_data) {
+        if ((rc = C->up(&f, C->h_marginal.data(), C->h_marginal.size()))) return rc;
+        S.marginal = f;
+        if ((rc = C->up(&f, C->h_conditional.data(), C->h_conditional.size()))) return rc;
+        S.conditional = f;
+        S.env_w = d.env_width;
+        S.env_h = d.env_height;
+        S.env_tex = C->env.obj;
+        S.has_env = 1;
+    }
+    // Morton box: the first instance's mesh bounds padded by 1e-5 (EPSILON of
+    // include/utilities.h:16), in that instance's object space
+    if (NI > 0) {
+        const float* mb = &mesh_box[size_t(d.instances[0].mesh) * 6];
+        for (int a = 0; a < 3; ++a) {
+            S.morton_bmin[a] = mb[a] - 0.00001f;
+            S.morton_bmax[a] = mb[3 + a] + 0.00001f;
+        }
+    }
+    return LUX_OK;
+}
+
+int alloc_wave(lux_ctx* C, int max_paths) {
+    DevWave& W = C->W;
+    std::memset(&W, 0, sizeof(W));
+    size_t n = size_t(max_paths);
+    int rc;
+    if ((rc = C->alloc(&W.s0, n)) || (rc = C->alloc(&W.s1, n)) || (rc = C->alloc(&W.s2, n)) ||
+        (rc = C->alloc(&W.s3, n)) || (rc = C->alloc(&W.s4, n)) || (rc = C->alloc(&W.queue[0], n)) ||
+        (rc = C->alloc(&W.queue[1], n)) || (rc = C->alloc(&W.hit, n)) || (rc = C->alloc(&W.hit_prim, n)) ||
+        (rc = C->alloc(&W.sh_o, n)) || (rc = C->alloc(&W.sh_d, n)) || (rc = C->alloc(&W.sh_queue, n)) ||
+        (rc = C->alloc(&W.sh_hit, n)) || (rc = C->alloc(&W.sh_prim, n)) || (rc = C->alloc(&W.ctr, 1)) ||
+        (rc = C->alloc(&W.wave_iter, 4)))
+        return rc;
+    if (C->opt.ray_sorting) {
+        if ((rc = C->alloc(&W.keys, n)) || (rc = C->alloc(&W.keys_alt, n)) || (rc = C->alloc(&W.queue_alt, n))) return rc;
+        C->sort_temp_bytes = morton_sort_temp_bytes(max_paths);
+        char* t = nullptr;
+        if ((rc = C->alloc(&t, C->sort_temp_bytes))) return rc;
+        C->sort_temp = t;
+    }
+    W.npix = C->npix;
+    W.width = C->width;
+    W.height = C->height;
+    W.max_paths = max_paths;
+    return LUX_OK;
+}
+
+// Enqueue one wave of ns samples starting at iteration W.wave_iter[0].
+int enqueue_wave(lux_ctx* C, int ns, const cudaEvent_t* ev) {
+    cudaStream_t st = C->stream;
+    DevWave& W = C->W;
+    const int n = ns * C->npix;
+    const int depth = C->dopt.trace_depth;
+    const int nee = C->dopt.env ? 2 : (C->dopt.dl ? 1 : 0);
+    int k = 0;
+    auto rec = [&]() {
+        if (ev) cudaEventRecord(ev[k], st);
+        ++k;
+    };
+    LUX_CUDA(cudaMemsetAsync(W.ctr, 0, sizeof(WaveCounters), st));
+    rec();
+    LUX_CUDA(launch_camera(C->S, W, C->dopt, C->cam, n, st));
+    rec();
+    for (int b = 0; b < depth; ++b) {
+        if (C->opt.ray_sorting) LUX_CUDA(launch_morton_sort(C->S, W, b, C->sort_temp, C->sort_temp_bytes, st));
+        rec();
+        LUX_CUDA(launch_trace(C->S, W, b, 0, nee, st));
+        if (nee) LUX_CUDA(launch_trace(C->S, W, b, nee == 2 ? 2 : 1, 0, st));
+        rec();
+        LUX_CUDA(launch_shade(C->S, W, C->dopt, b, (b + 1) < depth ? 1 : 0, st));
+        rec();
+    }
+    LUX_CUDA(launch_accumulate(W, C->image, C->comp, ns, C->opt.precision == LUX_PRECISION_COMPENSATED, st));
+    rec();
+    return LUX_OK;
+}
+
+int events_needed(const lux_ctx* C) { return 3 + 3 * C->dopt.trace_depth; }
+
+int run_waves(lux_ctx* C, int first_iter, int n_iter) {
+    if (n_iter <= 0) return LUX_OK;
+    cudaStream_t st = C->stream;
+    const int spw = C->spp_per_wave;
+    const int nwaves = (n_iter + spw - 1) / spw;
+    if (C->h_cap < nwaves) {
+        if (C->h_ctr) cudaFreeHost(C->h_ctr);
+        if (C->h_wave_iter) cudaFreeHost(C->h_wave_iter);
+        C->h_ctr = nullptr;
+        C->h_wave_iter = nullptr;
+        C->h_cap = 0;
+        LUX_CUDA(cudaMallocHost(&C->h_ctr, sizeof(WaveCounters) * nwaves));
+        LUX_CUDA(cudaMallocHost(&C->h_wave_iter, sizeof(int) * 2 * nwaves));
+        C->h_cap = nwaves;
+    }
+    const int epw = events_needed(C);
+    if (C->timing && int(C->kev.size()) < epw * nwaves) {
+        size_t have = C->kev.size();
+        C->kev.resize(size_t(epw) * nwaves);
+        for (size_t i = have; i < C->kev.size(); ++i) LUX_CUDA(cudaEventCreate(&C->kev[i]));
+    }
+    std::memset(&C->stats, 0, sizeof(C->stats));
+    LUX_CUDA(cudaEventRecord(C->ev[0], st));
+    for (int w = 0; w < nwaves; ++w) {
+        int it0 = first_iter + w * spw;
+        int ns = std::min(spw, first_iter + n_iter - it0);
+        // the wave's first iteration reaches the camera kernel through a device word, so a
+        // captured graph stays valid for every wave of the same size
+        C->h_wave_iter[2 * w] = it0;
+        C->h_wave_iter[2 * w + 1] = ns;
+        LUX_CUDA(cudaMemcpyAsync(C->W.wave_iter, &C->h_wave_iter[2 * w], 2 * sizeof(int), cudaMemcpyHostToDevice, st));
+        if (C->opt.use_graph && !C->timing) {
+            auto it = C->graphs.find(ns);
+            if (it == C->graphs.end()) {
+                cudaGraph_t g;
+                LUX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                int rc = enqueue_wave(C, ns, nullptr);
+                cudaError_t ce = cudaStreamEndCapture(st, &g);
+                if (rc) return rc;
+                if (ce != cudaSuccess) return fail(LUX_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+                cudaGraphExec_t ge;
+                cudaError_t ie = cudaGraphInstantiate(&ge, g, 0);
+                cudaGraphDestroy(g);
+                if (ie != cudaSuccess) return fail(LUX_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+                it = C->graphs.emplace(ns, ge).first;
+            }
+            LUX_CUDA(cudaGraphLaunch(it->second, st));
+        } else {
+            int rc = enqueue_wave(C, ns, C->timing ? &C->kev[size_t(w) * epw] : nullptr);
+            if (rc) return rc;
+        }
+        LUX_CUDA(cudaMemcpyAsync(&C->h_ctr[w], C->W.ctr, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st));
+    }
+    LUX_CUDA(cudaEventRecord(C->ev[1], st));
+    LUX_CUDA(cudaEventSynchronize(C->ev[1]));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, C->ev[0], C->ev[1]);
+    C->stats.ms_total = ms;
+    const int depth = C->dopt.trace_depth;
+    const bool nee = C->dopt.dl || C->dopt.env;
+    const int sort_launches = 1 + 4 * 3;
+    for (int w = 0; w < nwaves; ++w) {
+        const WaveCounters& c = C->h_ctr[w];
+        if (c.error) return fail(LUX_ERR_UNSUPPORTED, "traversal stack overflow");
+        for (int b = 0; b < depth; ++b) {
+            C->stats.rays_radiance += c.count[b];
+            C->stats.path_bounces += c.count[b];
+            C->stats.rays_shadow += c.shadow[b];
+        }
+        int ns = std::min(spw, n_iter - w * spw);
+        C->stats.samples += double(ns) * C->npix;
+        C->stats.launches_camera += 1;
+        C->stats.launches_accum += 1;
+        C->stats.launches_trace += depth * (nee ? 2 : 1);
+        C->stats.launches_shade += depth;
+        C->stats.launches_sort += C->opt.ray_sorting ? depth * sort_launches : 0;
+        if (C->timing) {
+            const cudaEvent_t* e = &C->kev[size_t(w) * epw];
+            float t;
+            cudaEventElapsedTime(&t, e[0], e[1]);
+            C->stats.ms_camera += t;
+            for (int b = 0; b < depth; ++b) {
+                cudaEventElapsedTime(&t, e[1 + 3 * b], e[2 + 3 * b]);
+                C->stats.ms_sort += t;
+                cudaEventElapsedTime(&t, e[2 + 3 * b], e[3 + 3 * b]);
+                C->stats.ms_trace += t;
+                cudaEventElapsedTime(&t, e[3 + 3 * b], e[4 + 3 * b]);
+                C->stats.ms_shade += t;
+            }
+            cudaEventElapsedTime(&t, e[1 + 3 * depth], e[2 + 3 * depth]);
+            C->stats.ms_accum += t;
+        }
+    }
+    C->stats.kernel_launches = C->stats.launches_camera + C->stats.launches_accum + C->stats.launches_trace +
+                               C->stats.launches_shade + C->stats.launches_sort;
+    C->accumulated += n_iter;
+    return LUX_OK;
+}
+
+struct Tmp {
+    std::vector<void*> p;
+    ~Tmp() {
+        for (void* q : p) cudaFree(q);
+    }
+    template <class T>
+    T* get(size_t n) {
+        void* q = nullptr;
+        if (cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) return nullptr;
+        p.push_back(q);
+        return static_cast<T*>(q);
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+void lux_default_options(lux_options* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->color_mode = LUX_TONEMAP_ACES;
+    o->envmap_intensity = 1.0f;
+    o->use_graph = 1;
+    o->texture_storage = LUX_TEXSTORE_FLOAT;
+}
+
+const char* lux_last_error(void) { return g_err.c_str(); }
+
+int lux_init(const lux_scene_desc* scene, const lux_options* opt, lux_ctx** out) {
+    if (!out) return fail(LUX_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!scene) return fail(LUX_ERR_INVALID, "scene is NULL");
+    const lux_scene_desc& d = *scene;
+    if (d.num_instances <= 0 || d.num_meshes <= 0 || !d.meshes || !d.instances)
+        return fail(LUX_ERR_INVALID, "scene has no geometry");
+    if (d.num_materials <= 0 || !d.materials) return fail(LUX_ERR_INVALID, "scene has no materials");
+    if (d.camera.width <= 0 || d.camera.height <= 0) return fail(LUX_ERR_INVALID, "camera resolution must be positive");
+    if (d.num_textures < 0 || (d.num_textures > 0 && !d.textures)) return fail(LUX_ERR_INVALID, "bad texture list");
+    for (int i = 0; i < d.num_meshes; ++i) {
+        const lux_mesh_desc& m = d.meshes[i];
+        if (m.num_tris <= 0 || m.num_verts <= 0 || !m.positions || !m.indices)
+            return fail(LUX_ERR_INVALID, "mesh " + std::to_string(i) + " is empty");
+        for (int k = 0; k < m.num_tris * 3; ++k)
+            if (m.indices[k] >= uint32_t(m.num_verts))
+                return fail(LUX_ERR_INVALID, "mesh " + std::to_string(i) + " index out of range");
+    }
+    for (int i = 0; i < d.num_instances; ++i) {
+        if (d.instances[i].mesh < 0 || d.instances[i].mesh >= d.num_meshes || d.instances[i].material < 0 ||
+            d.instances[i].material >= d.num_materials)
+            return fail(LUX_ERR_INVALID, "instance " + std::to_string(i) + " references a missing mesh or material");
+    }
+    if (d.env_data && (d.env_width <= 0 || d.env_height <= 0 ||
+                       (d.env_format != LUX_TEX_RGBA32F && d.env_format != LUX_TEX_RGBA16F)))
+        return fail(LUX_ERR_INVALID, "environment map must be RGBA32F or RGBA16F with a positive size");
+    lux_options o;
+    if (opt) o = *opt;
+    else lux_default_options(&o);
+    if (o.texture_storage < LUX_TEXSTORE_FLOAT || o.texture_storage > LUX_TEXSTORE_HALF)
+        return fail(LUX_ERR_INVALID, "unknown texture storage");
+    int tdepth = o.trace_depth > 0 ? o.trace_depth : d.trace_depth;
+    if (tdepth <= 0 || tdepth > kMaxDepth) return fail(LUX_ERR_INVALID, "trace depth must be in 1..64");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(LUX_ERR_NO_DEVICE, "no CUDA device");
+    if (o.device < 0 || o.device >= ndev) return fail(LUX_ERR_INVALID, "device ordinal out of range");
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, o.device);
+    if (prop.major < 10) return fail(LUX_ERR_NO_DEVICE, "an sm_100 device is required");
+    LUX_CUDA(cudaSetDevice(o.device));
+    lux_ctx* C = new lux_ctx();
+    C->device = o.device;
+    C->opt = o;
+    C->dopt.dl = o.direct_light_sampling ? 1 : 0;
+    C->dopt.env = o.env_importance_sampling ? 1 : 0;
+    C->dopt.env_intensity = o.envmap_intensity;
+    C->dopt.trace_depth = tdepth;
+    C->dopt.color_mode = o.color_mode;
+    C->dopt.precision = o.precision;
+    C->width = d.camera.width;
+    C->height = d.camera.height;
+    C->npix = C->width * C->height;
+    const lux_camera_desc& cd = d.camera;
+    for (int a = 0; a < 3; ++a) {
+        C->cam.pos[a] = cd.position[a];
+        C->cam.view[a] = cd.view[a];
+        C->cam.right[a] = cd.right[a];
+        C->cam.up[a] = cd.up[a];
+    }
+    C->cam.pixel_length[0] = cd.pixel_length[0];
+    C->cam.pixel_length[1] = cd.pixel_length[1];
+    C->cam.width = cd.width;
+    C->cam.height = cd.height;
+    auto bail = [&](int rc) {
+        std::string keep = g_err;
+        lux_free(C);
+        g_err = keep;
+        return rc;
+    };
+    if (o.stream) {
+        C->stream = static_cast<cudaStream_t>(o.stream);
+    } else {
+        if (cudaStreamCreateWithFlags(&C->stream, cudaStreamNonBlocking) != cudaSuccess)
+            return bail(fail(LUX_ERR_CUDA, "cudaStreamCreate failed"));
+        C->own_stream = true;
+    }
+    int rc = build_scene(C, d);
+    if (rc) return bail(rc);
+    // samples kept in flight together: about 8M paths, at least one sample
+    int spw = o.spp_per_wave > 0 ? o.spp_per_wave : std::max(1, (8 << 20) / C->npix);
+    spw = std::max(1, std::min(spw, 1 << 16));
+    C->spp_per_wave = spw;
+    if ((rc = alloc_wave(C, spw * C->npix))) return bail(rc);
+    if ((rc = C->alloc(&C->image, size_t(C->npix) * 3))) return bail(rc);
+    if (o.precision == LUX_PRECISION_COMPENSATED && (rc = C->alloc(&C->comp, size_t(C->npix) * 3))) return bail(rc);
+    if ((rc = C->alloc(&C->rgba, size_t(C->npix) * 4))) return bail(rc);
+    if (cudaMemset(C->image, 0, size_t(C->npix) * 3 * sizeof(float)) != cudaSuccess)
+        return bail(fail(LUX_ERR_CUDA, "memset"));
+    if (C->comp) cudaMemset(C->comp, 0, size_t(C->npix) * 3 * sizeof(float));
+    cudaEventCreate(&C->ev[0]);
+    cudaEventCreate(&C->ev[1]);
+    // occupancy queries happen here, never inside a stream capture
+    for (int m = 0; m < 3; ++m) trace_grid_blocks(m);
+    shade_grid_blocks();
+    if (cudaDeviceSynchronize() != cudaSuccess) return bail(fail(LUX_ERR_CUDA, cudaGetErrorString(cudaGetLastError())));
+    *out = C;
+    return LUX_OK;
+}
+
+int lux_render(lux_ctx* C, int first_iter, int n_iter) {
+    if (!C) return fail(LUX_ERR_STATE, "context is NULL");
+    if (first_iter < 1 || n_iter < 0) return fail(LUX_ERR_INVALID, "iterations are 1-based and n_iter >= 0");
+    cudaSetDevice(C->device);
+    return run_waves(C, first_iter, n_iter);
+}
+
+int lux_render_iter(lux_ctx* C, int iter, uint8_t* rgba8_dev) {
+    if (!C) return fail(LUX_ERR_STATE, "context is NULL");
+    if (iter < 1) return fail(LUX_ERR_INVALID, "iter is 1-based");
+    cudaSetDevice(C->device);
+    int save = C->spp_per_wave;
+    C->spp_per_wave = 1;
+    int rc = run_waves(C, iter, 1);
+    C->spp_per_wave = save;
+    if (rc) return rc;
+    if (rgba8_dev) {
+        LUX_CUDA(launch_tonemap(C->image, rgba8_dev, C->npix, float(iter), C->opt.color_mode, C->stream));
+        LUX_CUDA(cudaStreamSynchronize(C->stream));
+    }
+    return LUX_OK;
+}
+
+int lux_copy_image(lux_ctx* C, float* rgb_host) {
+    if (!C || !rgb_host) return fail(LUX_ERR_INVALID, "NULL argument");
+    cudaSetDevice(C->device);
+    LUX_CUDA(cudaMemcpyAsync(rgb_host, C->image, size_t(C->npix) * 3 * sizeof(float), cudaMemcpyDeviceToHost, C->stream));
+    LUX_CUDA(cudaStreamSynchronize(C->stream));
+    return LUX_OK;
+}
+
+int lux_copy_rgba8(lux_ctx* C, uint8_t* rgba_host) {
+    if (!C || !rgba_host) return fail(LUX_ERR_INVALID, "NULL argument");
+    cudaSetDevice(C->device);
+    float it = float(std::max(1, C->accumulated));
+    LUX_CUDA(launch_tonemap(C->image, C->rgba, C->npix, it, C->opt.color_mode, C->stream));
+    LUX_CUDA(cudaMemcpyAsync(rgba_host, C->rgba, size_t(C->npix) * 4, cudaMemcpyDeviceToHost, C->stream));
+    LUX_CUDA(cudaStreamSynchronize(C->stream));
+    return LUX_OK;
+}
+
+int lux_reset(lux_ctx* C) {
+    if (!C) return fail(LUX_ERR_STATE, "context is NULL");
+    cudaSetDevice(C->device);
+    LUX_CUDA(cudaMemsetAsync(C->image, 0, size_t(C->npix) * 3 * sizeof(float), C->stream));
+    if (C->comp) LUX_CUDA(cudaMemsetAsync(C->comp, 0, size_t(C->npix) * 3 * sizeof(float), C->stream));
+    LUX_CUDA(cudaStreamSynchronize(C->stream));
+    C->accumulated = 0;
+    return LUX_OK;
+}
+
+int lux_set_camera(lux_ctx* C, const lux_camera_desc* cd) {
+    if (!C || !cd) return fail(LUX_ERR_INVALID, "NULL argument");
+    if (cd->width != C->width || cd->height != C->height) return fail(LUX_ERR_INVALID, "resolution cannot change");
+    for (int a = 0; a < 3; ++a) {
+        C->cam.pos[a] = cd->position[a];
+        C->cam.view[a] = cd->view[a];
+        C->cam.right[a] = cd->right[a];
+        C->cam.up[a] = cd->up[a];
+    }
+    C->cam.pixel_length[0] = cd->pixel_length[0];
+    C->cam.pixel_length[1] = cd->pixel_length[1];
+    // camera parameters are baked into captured graphs
+    for (auto& g : C->graphs) cudaGraphExecDestroy(g.second);
+    C->graphs.clear();
+    return lux_reset(C);
+}
+
+int lux_free(lux_ctx* C) {
+    if (!C) return LUX_OK;
+    cudaSetDevice(C->device);
+    if (C->stream) cudaStreamSynchronize(C->stream);
+    for (auto& g : C->graphs) cudaGraphExecDestroy(g.second);
+    for (auto& t : C->texs) {
+        if (t.obj) cudaDestroyTextureObject(t.obj);
+        if (t.arr) cudaFreeArray(t.arr);
+    }
+    if (C->env.obj) cudaDestroyTextureObject(C->env.obj);
+    if (C->env.arr) cudaFreeArray(C->env.arr);
+    for (void* p : C->allocs) cudaFree(p);
+    if (C->h_wave_iter) cudaFreeHost(C->h_wave_iter);
+    if (C->h_ctr) cudaFreeHost(C->h_ctr);
+    for (auto e : C->kev) cudaEventDestroy(e);
+    if (C->ev[0]) cudaEventDestroy(C->ev[0]);
+    if (C->ev[1]) cudaEventDestroy(C->ev[1]);
+    if (C->own_stream && C->stream) cudaStreamDestroy(C->stream);
+    delete C;
+    return LUX_OK;
+}
+
+int lux_enable_timing(lux_ctx* C, int on) {
+    if (!C) return fail(LUX_ERR_STATE, "context is NULL");
+    C->timing = on != 0;
+    return LUX_OK;
+}
+
+int lux_get_stats(lux_ctx* C, lux_stats* out) {
+    if (!C || !out) return fail(LUX_ERR_INVALID, "NULL argument");
+    *out = C->stats;
+    return LUX_OK;
+}
+
+// ---- kernel-level entry points -------------------------------------------------------
+int lux_trace_rays(lux_ctx* C, const float* rays, int n, int mode, int iter, uint32_t* hits) {
+    if (!C || (!rays && n > 0) || (!hits && n > 0) || n < 0 || mode < 0 || mode > 2)
+        return fail(LUX_ERR_INVALID, "bad arguments");
+    if (n == 0) return LUX_OK;
+    cudaSetDevice(C->device);
+    Tmp t;
+    float* dr = t.get<float>(size_t(n) * 8);
+    uint32_t* dh = t.get<uint32_t>(size_t(n) * 5);
+    int* fetch = t.get<int>(1);
+    if (!dr || !dh || !fetch) return fail(LUX_ERR_OOM, "temporary allocation failed");
+    LUX_CUDA(cudaMemcpyAsync(dr, rays, size_t(n) * 8 * sizeof(float), cudaMemcpyHostToDevice, C->stream));
+    LUX_CUDA(cudaMemsetAsync(fetch, 0, sizeof(int), C->stream));
+    LUX_CUDA(cudaMemsetAsync(C->W.ctr, 0, sizeof(WaveCounters), C->stream));
+    LUX_CUDA(launch_trace_ext(C->S, C->W, dr, dh, n, mode, iter, fetch, C->stream));
+    LUX_CUDA(cudaMemcpyAsync(hits, dh, size_t(n) * 5 * sizeof(uint32_t), cudaMemcpyDeviceToHost, C->stream));
+    WaveCounters hc;
+    LUX_CUDA(cudaMemcpyAsync(&hc, C->W.ctr, sizeof(hc), cudaMemcpyDeviceToHost, C->stream));
+    LUX_CUDA(cudaStreamSynchronize(C->stream));
+    if (hc.error) return fail(LUX_ERR_UNSUPPORTED, "traversal stack overflow");
+    return LUX_OK;
+}
+
+int lux_morton_keys(lux_ctx* C, const float* rays, int n, uint32_t* keys) {
+    if (!C || n < 0 || (n > 0 && (!rays || !keys))) return fail(LUX_ERR_INVALID, "bad arguments");
+    if (n == 0) return LUX_OK;
+    cudaSetDevice(C->device);
+    Tmp t;
+    float* dr = t.get<float>(size_t(n) * 8);
+    uint32_t* dk = t.get<uint32_t>(size_t(n));
+    if (!dr || !dk) return fail(LUX_ERR_OOM, "temporary allocation failed");
+    LUX_CUDA(cudaMemcpyAsync(dr, rays, size_t(n) * 8 * sizeof(float), cudaMemcpyHostToDevice, C->stream));
+    LUX_CUDA(launch_morton_ext(C->S, dr, dk, n, C->stream));
+    LUX_CUDA(cudaMemcpyAsync(keys, dk, size_t(n) * sizeof(uint32_t), cudaMemcpyDeviceToHost, C->stream));
+    LUX_CUDA(cudaStreamSynchronize(C->stream));
+    return LUX_OK;
+}
+
+int lux_shade_step(lux_ctx* C, int iter, int depth, int compact, float* paths, int n, const uint32_t* hits,
+                   int* survivors, int* n_out) {
+    if (!C || n < 0 || !n_out || (n > 0 && (!paths || !hits || !survivors))) return fail(LUX_ERR_INVALID, "bad arguments");
+    *n_out = 0;
+    if (n == 0) return LUX_OK;
+    cudaSetDevice(C->device);
+    Tmp t;
+    float* dp = t.get<float>(size_t(n) * LUX_PS_FLOATS);
+    uint32_t* dh = t.get<uint32_t>(size_t(n) * 10);
+    int* ds = t.get<int>(size_t(n));
+    int* dn = t.get<int>(1);
+    if (!dp || !dh || !ds || !dn) return fail(LUX_ERR_OOM, "temporary allocation failed");
+    LUX_CUDA(cudaMemcpyAsync(dp, paths, size_t(n) * LUX_PS_FLOATS * sizeof(float), cudaMemcpyHostToDevice, C->stream));
+    LUX_CUDA(cudaMemcpyAsync(dh, hits, size_t(n) * 10 * sizeof(uint32_t), cudaMemcpyHostToDevice, C->stream));
+    LUX_CUDA(cudaMemsetAsync(dn, 0, sizeof(int), C->stream));
+    LUX_CUDA(launch_shade_ext(C->S, C->dopt, dp, dh, n, iter, depth, compact, ds, dn, C->stream));
+    LUX_CUDA(cudaMemcpyAsync(paths, dp, size_t(n) * LUX_PS_FLOATS * sizeof(float), cudaMemcpyDeviceToHost, C->stream));
+    LUX_CUDA(cudaMemcpyAsync(n_out, dn, sizeof(int), cudaMemcpyDeviceToHost, C->stream));
+    LUX_CUDA(cudaStreamSynchronize(C->stream));
+    LUX_CUDA(cudaMemcpy(survivors, ds, size_t(*n_out) * sizeof(int), cudaMemcpyDeviceToHost));
+    return LUX_OK;
+}
+
+int lux_light_samples(lux_ctx* C, int iter, int depth, const int* pixels, int n, float* out) {
+    if (!C || n < 0 || (n > 0 && (!pixels || !out))) return fail(LUX_ERR_INVALID, "bad arguments");
+    if (n == 0) return LUX_OK;
+    cudaSetDevice(C->device);
+    Tmp t;
+    int* dp = t.get<int>(size_t(n));
+    float* dout = t.get<float>(size_t(n) * 6);
+    if (!dp || !dout) return fail(LUX_ERR_OOM, "temporary allocation failed");
+    LUX_CUDA(cudaMemcpyAsync(dp, pixels, size_t(n) * sizeof(int), cudaMemcpyHostToDevice, C->stream));
+    LUX_CUDA(launch_light_ext(C->S, C->dopt, iter, depth, dp, n, dout, C->stream));
+    LUX_CUDA(cudaMemcpyAsync(out, dout, size_t(n) * 6 * sizeof(float), cudaMemcpyDeviceToHost, C->stream));
+    LUX_CUDA(cudaStreamSynchronize(C->stream));
+    return LUX_OK;
+}
+
+int lux_get_cdfs(lux_ctx* C, float* ep, float* tp, float* mg, float* cd, float* ta) {
+    if (!C) return fail(LUX_ERR_STATE, "context is NULL");
+    cudaSetDevice(C->device);
+    DevScene& S = C->S;
+    if (ep && S.num_emissive) LUX_CUDA(cudaMemcpy(ep, S.emissive_prefix, C->h_emissive_prefix.size() * 4, cudaMemcpyDeviceToHost));
+    if (tp && !C->h_tri_prefix.empty()) LUX_CUDA(cudaMemcpy(tp, S.tri_prefix, C->h_tri_prefix.size() * 4, cudaMemcpyDeviceToHost));
+    if (mg && S.has_env) LUX_CUDA(cudaMemcpy(mg, S.marginal, C->h_marginal.size() * 4, cudaMemcpyDeviceToHost));
+    if (cd && S.has_env) LUX_CUDA(cudaMemcpy(cd, S.conditional, C->h_conditional.size() * 4, cudaMemcpyDeviceToHost));
+    if (ta) *ta = S.total_area;
+    return LUX_OK;
+}
+
+int lux_rng_stream(int iter, int index, int depth, int n, float* out) {
+    if (n < 0 || (n > 0 && !out)) return fail(LUX_ERR_INVALID, "bad arguments");
+    if (n == 0) return LUX_OK;
+    Tmp t;
+    float* d = t.get<float>(size_t(n));
+    if (!d) return fail(LUX_ERR_OOM, "temporary allocation failed");
+    LUX_CUDA(launch_rng_ext(iter, index, depth, n, d, 0));
+    LUX_CUDA(cudaMemcpy(out, d, size_t(n) * sizeof(float), cudaMemcpyDeviceToHost));
+    return LUX_OK;
+}
+
+int lux_sample_texture(lux_ctx* C, int tex, const float* uv, int n, float* out) {
+    if (!C || n < 0 || (n > 0 && (!uv || !out))) return fail(LUX_ERR_INVALID, "bad arguments");
+    if (tex < -1 || tex >= int(C->texs.size())) return fail(LUX_ERR_INVALID, "texture index out of range");
+    if (tex == -1 && !C->S.has_env) return fail(LUX_ERR_INVALID, "no environment map");
+    if (n == 0) return LUX_OK;
+    cudaSetDevice(C->device);
+    Tmp t;
+    float* du = t.get<float>(size_t(n) * 2);
+    float* dout = t.get<float>(size_t(n) * 4);
+    if (!du || !dout) return fail(LUX_ERR_OOM, "temporary allocation failed");
+    LUX_CUDA(cudaMemcpyAsync(du, uv, size_t(n) * 2 * sizeof(float), cudaMemcpyHostToDevice, C->stream));
+    LUX_CUDA(launch_tex_ext(tex < 0 ? C->env.obj : C->texs[tex].obj, du, n, dout, C->stream));
+    LUX_CUDA(cudaMemcpyAsync(out, dout, size_t(n) * 4 * sizeof(float), cudaMemcpyDeviceToHost, C->stream));
+    LUX_CUDA(cudaStreamSynchronize(C->stream));
+    return LUX_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,145 @@
+// device_scene.h -- HBM layout of a resident scene and of one wavefront, shared by the host
+// side (context.cpp) and the kernels.
+//
+// Scene (read-only during rendering):
+//   nodes   BVH8 nodes (80 B, bvh8.h) of every mesh's BLAS, then the TLAS over instances
+//   prims   3 x float4 per leaf primitive record in BVH order: (v0, prim id), e1, e2 with
+//           e1 = v1 - v0 and e2 = v2 - v0 rounded once on the host, exactly the values the
+//           Moller-Trumbore test of src/intersections/mesh_isect.cu:79-82 computes
+//   insts   per instance: object<->world matrices, mesh bases, material, flags
+//   pos/nrm/uv/idx  shading attributes in the input order (single index stream)
+//   mats    uber-shader materials with bound texture objects
+//   light tables: emissive-area CDF, per-emissive-instance triangle CDFs, HDRI CDFs
+// Wavefront (per path id, SoA of float4 so each field is one 16-byte load):
+//   s0 = origin, last_pdf    s1 = direction, flags    s2 = throughput, pixel
+//   s3 = radiance, iteration s4 = NEE sample (DL point or env direction)
+// plus two path-id queues, per-slot hit records and the shadow-ray queue.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace lux {
+
+enum InstFlags : int { kInstHasNormals = 1, kInstHasUVs = 2, kInstAnyHit = 4 };
+
+struct DevInstance {
+    float M[12];      // object -> world, columns 0..3 of the 4x4 (rows 0..2)
+    float Minv[12];   // world -> object
+    float MinvT[12];  // inverse transpose (normal transform)
+    int mesh;
+    int material;
+    uint32_t blas_root;   // node index of the mesh's BLAS root
+    uint32_t prim_base;   // first primitive record of the mesh
+    uint32_t vert_base;   // first vertex of the mesh in pos/nrm/uv
+    uint32_t idx_base;    // first index triplet of the mesh
+    int flags;            // InstFlags
+    int num_tris;
+};
+
+enum MatFlags : int { kMatAlbedoTex = 1, kMatEmissiveTex = 2, kMatNormalTex = 4, kMatMRTex = 8 };
+
+struct DevTexTransform {
+    float offset[2];
+    float scale[2];
+    float rotation;
+};
+
+struct DevMaterial {
+    float color[3];
+    float alpha;
+    float emission[3];  // emission_color * emission_strength, rounded as the shader does
+    float roughness;
+    float metallic;
+    float transmission;
+    float ior;
+    float alpha_cutoff;
+    int alpha_mode;
+    int flags;  // MatFlags
+    int pad[2];
+    unsigned long long albedo_tex, emissive_tex, normal_tex, mr_tex;
+    DevTexTransform albedo_tt, emissive_tt, normal_tt, mr_tt;
+};
+
+struct DevScene {
+    const uint4* nodes;
+    const float4* prims;
+    const DevInstance* insts;
+    const uint32_t* tlas_prims;  // TLAS leaf records -> instance index
+    uint32_t tlas_root;
+    int num_insts;
+    const float* pos;
+    const float* nrm;
+    const float* uv;
+    const uint32_t* idx;
+    const DevMaterial* mats;
+    // light sampling tables (src/scene/scene_precompute.cpp:22-124)
+    const int* emissive_inst;
+    const float* emissive_prefix;
+    const float* tri_prefix;      // concatenated per emissive instance
+    const int* tri_prefix_off;    // offset of each emissive instance's table
+    int num_emissive;
+    float total_area;
+    const float* marginal;
+    const float* conditional;
+    int env_w, env_h;
+    unsigned long long env_tex;
+    int has_env;
+    float morton_bmin[3], morton_bmax[3];
+};
+
+struct DevCamera {
+    float pos[3], view[3], right[3], up[3];
+    float pixel_length[2];
+    int width, height;
+};
+
+struct DevOptions {
+    int dl;             // -dmis
+    int env;            // -emis
+    float env_intensity;
+    int trace_depth;
+    int color_mode;
+    int precision;
+};
+
+// Per-bounce device counters, zeroed once per wave (one memset):
+//   count[b]     queue length entering bounce b (count[0] = paths of the wave)
+//   shadow[b]    shadow rays queued at bounce b
+//   fetch_r[b], fetch_s[b]  work-fetch cursors of the persistent trace kernels
+//   error        sticky error word (bit 0: traversal stack overflow)
+constexpr int kMaxDepth = 64;
+struct WaveCounters {
+    int count[kMaxDepth + 1];
+    int shadow[kMaxDepth];
+    int fetch_r[kMaxDepth];
+    int fetch_s[kMaxDepth];
+    int error;
+    int pad[3];
+};
+
+struct DevWave {
+    float4* s0;
+    float4* s1;
+    float4* s2;
+    float4* s3;
+    float4* s4;
+    int* queue[2];
+    float4* hit;      // per slot: t, u, v, instance (int bits)
+    int* hit_prim;    // per slot
+    float4* sh_o;     // per slot: shadow origin, tmax
+    float4* sh_d;     // per slot: shadow direction
+    int* sh_queue;    // slots with a shadow ray
+    float4* sh_hit;   // per slot: DL hit t, u, v, instance; env: occlusion in .x
+    int* sh_prim;
+    uint32_t* keys;   // Morton keys (ray sorting)
+    uint32_t* keys_alt;
+    int* queue_alt;
+    WaveCounters* ctr;
+    int* wave_iter;   // [0] first iteration of the wave, [1] samples in the wave
+    int npix;         // pixels of the job
+    int width, height;
+    int max_paths;
+};
+
+}  // namespace lux

@@ -1,0 +1,47 @@
+// launch.h -- host-callable launchers of the kernels (defined in trace.cu, shade.cu, sort.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include "device_scene.h"
+
+namespace lux {
+
+constexpr int kTraceBlock = 128;
+constexpr int kShadeBlock = 128;
+
+int trace_grid_blocks(int mode);
+int shade_grid_blocks();
+
+// persistent trace of bounce `bounce`: mode 0 radiance (queues shadow rays when nee != 0:
+// 1 DL, 2 env), 1 DL shadow rays, 2 env occlusion rays
+cudaError_t launch_trace(const DevScene& S, const DevWave& W, int bounce, int mode, int nee, cudaStream_t st);
+// trace caller rays (device buffers), n * 8 floats -> n * 5 words; fetch is a zeroed int
+cudaError_t launch_trace_ext(const DevScene& S, const DevWave& W, const float* rays, uint32_t* hits, int n, int mode,
+                             int iter, int* fetch, cudaStream_t st);
+
+// camera rays for paths [0, n) of the wave (+ NEE sample of bounce 0), queue 0 = identity
+cudaError_t launch_camera(const DevScene& S, const DevWave& W, const DevOptions& O, const DevCamera& cam, int n,
+                          cudaStream_t st);
+// shade bounce `bounce` (depth = bounce + 1 after the increment of src/pathtrace.cu:264)
+cudaError_t launch_shade(const DevScene& S, const DevWave& W, const DevOptions& O, int bounce, int compact,
+                         cudaStream_t st);
+// image[p] (+comp) += radiance of every sample of the wave, in sample order
+cudaError_t launch_accumulate(const DevWave& W, float* image, float* comp, int nsamples, int compensated,
+                              cudaStream_t st);
+cudaError_t launch_tonemap(const float* image, uint8_t* rgba, int npix, float iter, int color_mode, cudaStream_t st);
+
+// Morton keys of the bounce's queue and a stable LSD radix sort of the queue by key
+cudaError_t launch_morton_sort(const DevScene& S, DevWave& W, int bounce, void* temp, size_t temp_bytes,
+                               cudaStream_t st);
+size_t morton_sort_temp_bytes(int max_paths);
+cudaError_t launch_morton_ext(const DevScene& S, const float* rays, uint32_t* keys, int n, cudaStream_t st);
+
+// kernel-level parity entry points (device buffers)
+cudaError_t launch_shade_ext(const DevScene& S, const DevOptions& O, float* paths, const uint32_t* hits, int n,
+                             int iter, int depth, int compact, int* survivors, int* n_out, cudaStream_t st);
+cudaError_t launch_light_ext(const DevScene& S, const DevOptions& O, int iter, int depth, const int* pixels, int n,
+                             float* out, cudaStream_t st);
+cudaError_t launch_rng_ext(int iter, int index, int depth, int n, float* out, cudaStream_t st);
+cudaError_t launch_tex_ext(unsigned long long tex, const float* uv, int n, float* out, cudaStream_t st);
+
+}  // namespace lux

@@ -1,0 +1,548 @@
+// trace.cu -- ray traversal of the two-level compressed 8-wide BVH on sm_100a.
+//
+// Replaces the reference's OptiX launch (src/pathtrace.cu:238-258, device programs in
+// src/optixshaders/optix_triangle.cu:52-366) and its disabled software path
+// (src/kernels/compute_intersections.cu:6-87, src/intersections/mesh_isect.cu:6-149).
+//
+// Design:
+//  * persistent warps: lanes without a ray take the next ones from a global cursor with one
+//    atomicAdd per warp (ballot/popc), and a warp leaves its inner loop to refill as soon as
+//    fewer than kRefill lanes are still traversing (Aila & Laine's while-while with dynamic
+//    fetch);
+//  * the traversal stack keeps its top kShStack entries in shared memory (one column per
+//    thread, conflict-free) and spills deeper entries to local memory;
+//  * node groups / triangle groups as in Ylitie et al. 2017: a stack entry is a node's
+//    remaining internal-child hits (ordered by ray octant) or a set of leaf records;
+//  * two levels: the TLAS is traversed with the world ray; a TLAS leaf pushes a marker and
+//    continues in the instance's BLAS with the object-space ray the reference uses
+//    (inverseTransform * (o,1), (d,0), src/intersections/mesh_isect.cu:15-16);
+//  * the triangle test is the reference's Moller-Trumbore (mesh_isect.cu:78-137) with every
+//    operation rounded on its own, so t, u, v and the hit triangle match the CPU oracle bit
+//    for bit on the same rays; equal t is resolved toward the lowest (instance, primitive);
+//  * alpha mask / blend any-hit (optix_triangle.cu:317-366) is evaluated on candidate hits of
+//    instances whose material is not opaque.
+// Box tests are conservative: child boxes are quantised outward at build time and the slab
+// interval is widened by a relative 2^-19, so no triangle the exact test accepts is skipped.
+
+#include "device_scene.h"
+#include "device_math.cuh"
+#include "bvh8.h"
+#include "launch.h"
+
+namespace lux {
+
+namespace {
+
+constexpr int kShStack = 16;
+constexpr int kLocStack = 48;
+constexpr int kRefill = 20;
+constexpr uint32_t kTagMask = 3u << 30;
+constexpr uint32_t kTagNode = 0u;
+constexpr uint32_t kTagInst = 2u << 30;
+constexpr uint32_t kTagMarker = 3u << 30;
+constexpr float kLo = 1.0f - 1.0f / 524288.0f;
+constexpr float kHi = 1.0f + 1.0f / 524288.0f;
+
+struct TRay {
+    f3 o, d, idir;
+    uint32_t oct;
+};
+
+LUX_DI TRay make_ray(f3 o, f3 d) {
+    TRay r;
+    r.o = o;
+    r.d = d;
+    r.idir = mk(__frcp_rn(d.x), __frcp_rn(d.y), __frcp_rn(d.z));
+    r.oct = (__float_as_uint(r.idir.x) >> 31) | ((__float_as_uint(r.idir.y) >> 31) << 1) |
+            ((__float_as_uint(r.idir.z) >> 31) << 2);
+    return r;
+}
+
+LUX_DI float ubyte(uint32_t w, int s) { return __uint_as_float(0x4B000000u | ((w >> (8 * s)) & 0xffu)) - 8388608.0f; }
+
+// Intersect the 8 child boxes of node ni. Returns internal-child hits as a key mask
+// (bit (slot ^ oct)), the leaf primitive mask (bit offset), child_base and tri_base.
+LUX_DI void visit_node(const uint4* __restrict__ nodes, uint32_t ni, const TRay& r, float tmax, uint32_t& keys,
+                       uint32_t& imask, uint32_t& child_base, uint32_t& tri_base, uint32_t& trimask) {
+    const uint4* n = nodes + size_t(ni) * 5;
+    uint4 w0 = __ldg(n + 0), w1 = __ldg(n + 1), w2 = __ldg(n + 2), w3 = __ldg(n + 3), w4 = __ldg(n + 4);
+    float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
+    float sx = __uint_as_float((w0.w & 0xffu) << 23);
+    float sy = __uint_as_float(((w0.w >> 8) & 0xffu) << 23);
+    float sz = __uint_as_float(((w0.w >> 16) & 0xffu) << 23);
+    imask = w0.w >> 24;
+    child_base = w1.x;
+    tri_base = w1.y;
+    float ax = sx * r.idir.x, ay = sy * r.idir.y, az = sz * r.idir.z;
+    float bx = (px - r.o.x) * r.idir.x, by = (py - r.o.y) * r.idir.y, bz = (pz - r.o.z) * r.idir.z;
+    // near/far quantised planes per axis, by ray octant
+    const bool fx = r.oct & 1, fy = r.oct & 2, fz = r.oct & 4;
+    uint32_t nx0 = fx ? w3.z : w2.x, nx1 = fx ? w3.w : w2.y, fx0 = fx ? w2.x : w3.z, fx1 = fx ? w2.y : w3.w;
+    uint32_t ny0 = fy ? w4.x : w2.z, ny1 = fy ? w4.y : w2.w, fy0 = fy ? w2.z : w4.x, fy1 = fy ? w2.w : w4.y;
+    uint32_t nz0 = fz ? w4.z : w3.x, nz1 = fz ? w4.w : w3.y, fz0 = fz ? w3.x : w4.z, fz1 = fz ? w3.y : w4.w;
+    keys = 0;
+    trimask = 0;
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+        const int b = s & 3;
+        uint32_t wnx = s < 4 ? nx0 : nx1, wny = s < 4 ? ny0 : ny1, wnz = s < 4 ? nz0 : nz1;
+        uint32_t wfx = s < 4 ? fx0 : fx1, wfy = s < 4 ? fy0 : fy1, wfz = s < 4 ? fz0 : fz1;
+        float tnx = fmaf(ubyte(wnx, b), ax, bx), tny = fmaf(ubyte(wny, b), ay, by), tnz = fmaf(ubyte(wnz, b), az, bz);
+        float tfx = fmaf(ubyte(wfx, b), ax, bx), tfy = fmaf(ubyte(wfy, b), ay, by), tfz = fmaf(ubyte(wfz, b), az, bz);
+        float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
+        float tf = fminf(fminf(tfx, tfy), fminf(tfz, tmax));
+        uint32_t meta = ((s < 4 ? w1.z : w1.w) >> (8 * b)) & 0xffu;
+        bool hit = (meta != 0u) && (tn * kLo <= tf * kHi);
+        if (hit) {
+            if (meta & 0x80u) {
+                keys |= 1u << (uint32_t(s) ^ r.oct);
+            } else {
+                uint32_t cnt = meta >> 5, off = meta & 31u;
+                trimask |= ((1u << cnt) - 1u) << off;
+            }
+        }
+    }
+}
+
+struct Best {
+    float t;
+    int inst, prim;
+    float u, v;
+};
+
+LUX_DI bool better(float t, int inst, int prim, const Best& b) {
+    if (b.inst < 0) return true;
+    if (t < b.t) return true;
+    return t == b.t && (inst < b.inst || (inst == b.inst && prim < b.prim));
+}
+
+// Moller-Trumbore exactly as src/intersections/mesh_isect.cu:78-115, single-rounded ops.
+LUX_DI bool mt_test(const float4* __restrict__ prims, uint32_t rec, const TRay& r, float& t, float& u, float& v,
+                    int& prim) {
+    const float4* q = prims + size_t(rec) * 3;
+    float4 a4 = __ldg(q), e14 = __ldg(q + 1), e24 = __ldg(q + 2);
+    prim = __float_as_int(a4.w);
+    const f3 e1 = mk(e14.x, e14.y, e14.z), e2 = mk(e24.x, e24.y, e24.z);
+    const f3 d = r.d;
+    // cross(d, e2) = (d.y*e2.z - e2.y*d.z, d.z*e2.x - e2.z*d.x, d.x*e2.y - e2.x*d.y)
+    f3 c = mk(__fsub_rn(__fmul_rn(d.y, e2.z), __fmul_rn(e2.y, d.z)), __fsub_rn(__fmul_rn(d.z, e2.x), __fmul_rn(e2.z, d.x)),
+              __fsub_rn(__fmul_rn(d.x, e2.y), __fmul_rn(e2.x, d.y)));
+    float det = __fadd_rn(__fadd_rn(__fmul_rn(e1.x, c.x), __fmul_rn(e1.y, c.y)), __fmul_rn(e1.z, c.z));
+    if (det > -kMT_EPS && det < kMT_EPS) return false;
+    float inv = __frcp_rn(det);
+    f3 a = mk(__fsub_rn(r.o.x, a4.x), __fsub_rn(r.o.y, a4.y), __fsub_rn(r.o.z, a4.z));
+    u = __fmul_rn(inv, __fadd_rn(__fadd_rn(__fmul_rn(a.x, c.x), __fmul_rn(a.y, c.y)), __fmul_rn(a.z, c.z)));
+    if (u < -kMT_EPS || u > 1.0f + kMT_EPS) return false;
+    // cross(a, e1)
+    c = mk(__fsub_rn(__fmul_rn(a.y, e1.z), __fmul_rn(e1.y, a.z)), __fsub_rn(__fmul_rn(a.z, e1.x), __fmul_rn(e1.z, a.x)),
+           __fsub_rn(__fmul_rn(a.x, e1.y), __fmul_rn(e1.x, a.y)));
+    v = __fmul_rn(inv, __fadd_rn(__fadd_rn(__fmul_rn(d.x, c.x), __fmul_rn(d.y, c.y)), __fmul_rn(d.z, c.z)));
+    float uv = __fadd_rn(u, v);
+    if ((v < 0.0f && fabsf(v) > kMT_EPS) || (uv > 1.0f && fabsf(__fsub_rn(uv, 1.0f)) > kMT_EPS)) return false;
+    t = __fmul_rn(inv, __fadd_rn(__fadd_rn(__fmul_rn(e2.x, c.x), __fmul_rn(e2.y, c.y)), __fmul_rn(e2.z, c.z)));
+    return t > kMT_EPS;
+}
+
+// Any-hit program (src/optixshaders/optix_triangle.cu:317-366): true = accept the hit.
+LUX_DI bool alpha_accept(const DevScene& S, const DevInstance& I, int inst, int prim, float bu, float bv, f3 wdir,
+                         int pixel, int iter) {
+    const DevMaterial& m = S.mats[I.material];
+    if (m.alpha_mode == 0) return true;
+    float alpha = m.alpha;
+    if (m.flags & kMatAlbedoTex) {
+        float ux = 0.0f, uy = 0.0f;
+        if (I.flags & kInstHasUVs) {
+            const uint32_t* id = S.idx + (size_t(I.idx_base) + prim) * 3;
+            uint32_t i0 = I.vert_base + id[0], i1 = I.vert_base + id[1], i2 = I.vert_base + id[2];
+            float bA = 1.0f - bu - bv;
+            ux = bA * S.uv[i0 * 2] + bu * S.uv[i1 * 2] + bv * S.uv[i2 * 2];
+            uy = bA * S.uv[i0 * 2 + 1] + bu * S.uv[i1 * 2 + 1] + bv * S.uv[i2 * 2 + 1];
+        }
+        ux = ux * m.albedo_tt.scale[0];
+        uy = uy * m.albedo_tt.scale[1];
+        if (m.albedo_tt.rotation != 0.0f) {
+            float c = cosf(m.albedo_tt.rotation), s = sinf(m.albedo_tt.rotation);
+            float nx = c * ux - s * uy, ny = s * ux + c * uy;
+            ux = nx;
+            uy = ny;
+        }
+        ux = ux + m.albedo_tt.offset[0];
+        uy = uy + m.albedo_tt.offset[1];
+        float4 tx = tex2D<float4>(cudaTextureObject_t(m.albedo_tex), ux, uy);
+        alpha *= tx.w;
+    }
+    if (m.alpha_mode == 1) return !(alpha < m.alpha_cutoff);
+    uint32_t h = hash_u32(uint32_t(pixel) ^ hash_u32(uint32_t(iter)));
+    h = hash_u32(h ^ __float_as_uint(wdir.x));
+    h = hash_u32(h ^ __float_as_uint(wdir.y));
+    h = hash_u32(h ^ __float_as_uint(wdir.z));
+    h = hash_u32(h ^ uint32_t(inst));
+    h = hash_u32(h ^ uint32_t(prim));
+    float rnd = float(h >> 8) * (1.0f / 16777216.0f);
+    return !(rnd >= alpha);
+}
+
+// Traversal state of one lane.
+struct Lane {
+    TRay world, cur;
+    float tmax;
+    Best best;
+    uint2 grp;          // current group
+    int sp;             // stack depth
+    int inst;           // current instance (-1 in the TLAS)
+    int inst_flags;
+    uint32_t inst_prim_base;
+    int pixel, iter;    // alpha-blend hash key
+    bool done;
+};
+
+template <int MODE>
+struct Tracer {
+    const DevScene& S;
+    uint2 (*sh)[kTraceBlock];  // shared stack [kShStack][block]
+    uint2 loc[kLocStack];
+    int tid;
+    int* err;
+
+    LUX_DI void push(Lane& L, uint2 e) {
+        if (L.sp < kShStack) sh[L.sp][tid] = e;
+        else if (L.sp < kShStack + kLocStack) loc[L.sp - kShStack] = e;
+        else {
+            atomicOr(err, 1);
+            return;
+        }
+        ++L.sp;
+    }
+    LUX_DI uint2 pop(Lane& L) {
+        --L.sp;
+        return L.sp < kShStack ? sh[L.sp][tid] : loc[L.sp - kShStack];
+    }
+
+    LUX_DI void start(Lane& L, f3 o, f3 d, float tmax) {
+        L.world = make_ray(o, d);
+        L.cur = L.world;
+        L.tmax = tmax;
+        L.best.t = -1.0f;
+        L.best.inst = -1;
+        L.best.prim = -1;
+        L.best.u = L.best.v = 0.0f;
+        L.sp = 0;
+        L.inst = -1;
+        L.inst_flags = 0;
+        L.done = false;
+        // root group: a single internal "child" = the TLAS root, at key oct (slot 0)
+        L.grp = make_uint2(S.tlas_root, kTagNode | (1u << 8) | (1u << L.cur.oct));
+    }
+
+    LUX_DI float limit(const Lane& L) const { return (MODE != 2 && L.best.inst >= 0) ? L.best.t : L.tmax; }
+
+    LUX_DI void enter_instance(Lane& L, int ii) {
+        const DevInstance& I = S.insts[ii];
+        f3 oo = xform(I.Minv, L.world.o, 1.0f);
+        f3 od = xform(I.Minv, L.world.d, 0.0f);
+        push(L, make_uint2(0u, kTagMarker));
+        L.cur = make_ray(oo, od);
+        L.inst = ii;
+        L.inst_flags = I.flags;
+        L.inst_prim_base = I.prim_base;
+        L.grp = make_uint2(I.blas_root, kTagNode | (1u << 8) | (1u << L.cur.oct));
+    }
+
+    LUX_DI void test_prims(Lane& L, uint32_t base, uint32_t mask) {
+        while (mask) {
+            int k = __ffs(mask) - 1;
+            mask &= mask - 1;
+            float t, u, v;
+            int prim;
+            if (!mt_test(S.prims, L.inst_prim_base + base + uint32_t(k), L.cur, t, u, v, prim)) continue;
+            if (!(t <= L.tmax)) continue;
+            if (MODE != 2 && !better(t, L.inst, prim, L.best)) continue;
+            if (L.inst_flags & kInstAnyHit) {
+                if (!alpha_accept(S, S.insts[L.inst], L.inst, prim, u, v, L.world.d, L.pixel, L.iter)) continue;
+            }
+            L.best.t = t;
+            L.best.inst = L.inst;
+            L.best.prim = prim;
+            L.best.u = u;
+            L.best.v = v;
+            if (MODE == 2) {
+                L.done = true;
+                return;
+            }
+        }
+    }
+
+    // One traversal step; sets L.done when the ray is finished.
+    LUX_DI void step(Lane& L) {
+        uint32_t tag = L.grp.y & kTagMask;
+        if (tag == kTagNode && (L.grp.y & 0xffu)) {
+            uint32_t keys = L.grp.y & 0xffu;
+            uint32_t key = __ffs(keys) - 1;
+            keys &= keys - 1;
+            uint32_t slot = key ^ L.cur.oct;
+            uint32_t imask = (L.grp.y >> 8) & 0xffu;
+            uint32_t child = L.grp.x + __popc(imask & ((1u << slot) - 1u));
+            if (keys) push(L, make_uint2(L.grp.x, (L.grp.y & ~0xffu) | keys));
+            uint32_t nkeys, nimask, cbase, tbase, tmask;
+            visit_node(S.nodes, child, L.cur, limit(L), nkeys, nimask, cbase, tbase, tmask);
+            if (tmask) {
+                if (L.inst >= 0) {
+                    test_prims(L, tbase, tmask);
+                    if (L.done) return;
+                } else {
+                    // TLAS leaves: instances, handled as a group after the node group
+                    if (nkeys) push(L, make_uint2(cbase, kTagNode | (nimask << 8) | nkeys));
+                    L.grp = make_uint2(tbase, kTagInst | tmask);
+                    return;
+                }
+            }
+            L.grp = make_uint2(cbase, kTagNode | (nimask << 8) | nkeys);
+            return;
+        }
+        if (tag == kTagInst && (L.grp.y & 0xffffffu)) {
+            uint32_t m = L.grp.y & 0xffffffu;
+            int k = __ffs(m) - 1;
+            m &= m - 1;
+            int ii = int(__ldg(S.tlas_prims + L.grp.x + uint32_t(k)));
+            if (m) push(L, make_uint2(L.grp.x, kTagInst | m));
+            enter_instance(L, ii);
+            return;
+        }
+        // current group exhausted: pop
+        while (true) {
+            if (L.sp == 0) {
+                L.done = true;
+                return;
+            }
+            uint2 e = pop(L);
+            if ((e.y & kTagMask) == kTagMarker) {
+                L.cur = L.world;
+                L.inst = -1;
+                L.inst_flags = 0;
+                continue;
+            }
+            L.grp = e;
+            return;
+        }
+    }
+};
+
+struct TraceArgs {
+    DevScene S;
+    DevWave W;
+    int bounce;
+    int mode;    // 0 radiance, 1 DL shadow, 2 env shadow
+    int nee;     // radiance pass: 0 none, 1 DL, 2 env
+    const float* ext_rays;  // lux_trace_rays: rays given directly (n * 8 floats)
+    uint32_t* ext_hits;     // and hits written directly (n * 5 words)
+    int ext_n;
+    int ext_iter;
+    int* ext_fetch;
+};
+
+// World normal of a radiance hit as the closest-hit program computes it
+// (src/optixshaders/optix_triangle.cu:170-192,224): interpolated vertex normals when the
+// mesh has them, else the geometric normal, then the normal transform of the instance.
+LUX_DI f3 hit_world_normal(const DevScene& S, int inst, int prim, float bu, float bv) {
+    const DevInstance& I = S.insts[inst];
+    const uint32_t* id = S.idx + (size_t(I.idx_base) + prim) * 3;
+    uint32_t i0 = I.vert_base + __ldg(id), i1 = I.vert_base + __ldg(id + 1), i2 = I.vert_base + __ldg(id + 2);
+    f3 n;
+    if (I.flags & kInstHasNormals) {
+        float bA = __fsub_rn(__fsub_rn(1.0f, bu), bv);
+        f3 nA = ld3(S.nrm + i0 * 3), nB = ld3(S.nrm + i1 * 3), nC = ld3(S.nrm + i2 * 3);
+        f3 s = mk(__fadd_rn(__fadd_rn(__fmul_rn(bA, nA.x), __fmul_rn(bu, nB.x)), __fmul_rn(bv, nC.x)),
+                  __fadd_rn(__fadd_rn(__fmul_rn(bA, nA.y), __fmul_rn(bu, nB.y)), __fmul_rn(bv, nC.y)),
+                  __fadd_rn(__fadd_rn(__fmul_rn(bA, nA.z), __fmul_rn(bu, nB.z)), __fmul_rn(bv, nC.z)));
+        float l2 = __fadd_rn(__fadd_rn(__fmul_rn(s.x, s.x), __fmul_rn(s.y, s.y)), __fmul_rn(s.z, s.z));
+        float il = __fdiv_rn(1.0f, __fsqrt_rn(l2));
+        n = mk(__fmul_rn(s.x, il), __fmul_rn(s.y, il), __fmul_rn(s.z, il));
+    } else {
+        f3 A = ld3(S.pos + i0 * 3), B = ld3(S.pos + i1 * 3), C = ld3(S.pos + i2 * 3);
+        f3 e1 = mk(__fsub_rn(B.x, A.x), __fsub_rn(B.y, A.y), __fsub_rn(B.z, A.z));
+        f3 e2 = mk(__fsub_rn(C.x, A.x), __fsub_rn(C.y, A.y), __fsub_rn(C.z, A.z));
+        f3 c = mk(__fsub_rn(__fmul_rn(e1.y, e2.z), __fmul_rn(e2.y, e1.z)), __fsub_rn(__fmul_rn(e1.z, e2.x), __fmul_rn(e2.z, e1.x)),
+                  __fsub_rn(__fmul_rn(e1.x, e2.y), __fmul_rn(e2.x, e1.y)));
+        float l2 = __fadd_rn(__fadd_rn(__fmul_rn(c.x, c.x), __fmul_rn(c.y, c.y)), __fmul_rn(c.z, c.z));
+        float il = __fdiv_rn(1.0f, __fsqrt_rn(l2));
+        n = mk(__fmul_rn(c.x, il), __fmul_rn(c.y, il), __fmul_rn(c.z, il));
+    }
+    f3 w = xform(I.MinvT, n, 0.0f);
+    float l2 = __fadd_rn(__fadd_rn(__fmul_rn(w.x, w.x), __fmul_rn(w.y, w.y)), __fmul_rn(w.z, w.z));
+    float il = __fdiv_rn(1.0f, __fsqrt_rn(l2));
+    return mk(__fmul_rn(w.x, il), __fmul_rn(w.y, il), __fmul_rn(w.z, il));
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kTraceBlock, 4) k_trace(TraceArgs A) {
+    __shared__ uint2 stack[kShStack][kTraceBlock];
+    Tracer<MODE> T{A.S, stack, {}, int(threadIdx.x), &A.W.ctr->error};
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const bool ext = A.ext_rays != nullptr;
+    int total;
+    int* cursor;
+    if (ext) {
+        total = A.ext_n;
+        cursor = A.ext_fetch;
+    } else if (MODE == 0) {
+        total = *(volatile int*)&A.W.ctr->count[A.bounce];
+        cursor = &A.W.ctr->fetch_r[A.bounce];
+    } else {
+        total = *(volatile int*)&A.W.ctr->shadow[A.bounce];
+        cursor = &A.W.ctr->fetch_s[A.bounce];
+    }
+    Lane L;
+    bool active = false;
+    bool exhausted = false;  // warp-uniform: the cursor has passed the end of the work list
+    int item = 0;
+    while (true) {
+        unsigned need = __ballot_sync(FULL, !active);
+        if (need && !exhausted) {
+            int base = 0;
+            if (lane == 0) base = atomicAdd(cursor, __popc(need));
+            base = __shfl_sync(FULL, base, 0);
+            if (base + __popc(need) >= total) exhausted = true;
+            if (!active) {
+                int r = base + __popc(need & ((1u << lane) - 1u));
+                if (r < total) {
+                    item = r;
+                    f3 o, d;
+                    float tmax;
+                    L.pixel = 0;
+                    L.iter = 0;
+                    if (ext) {
+                        const float* ry = A.ext_rays + size_t(r) * 8;
+                        o = mk(ry[0], ry[1], ry[2]);
+                        d = mk(ry[4], ry[5], ry[6]);
+                        tmax = MODE == 1 ? ry[3] : 1e16f;
+                        L.pixel = __float_as_int(ry[7]);
+                        L.iter = A.ext_iter;
+                    } else if (MODE == 0) {
+                        int pid = A.W.queue[A.bounce & 1][r];
+                        float4 a = A.W.s0[pid], b = A.W.s1[pid];
+                        o = mk(a.x, a.y, a.z);
+                        d = mk(b.x, b.y, b.z);
+                        tmax = 1e16f;
+                        L.pixel = __float_as_int(A.W.s2[pid].w);
+                        L.iter = __float_as_int(A.W.s3[pid].w);
+                    } else {
+                        int slot = A.W.sh_queue[r];
+                        item = slot;
+                        float4 a = A.W.sh_o[slot], b = A.W.sh_d[slot];
+                        o = mk(a.x, a.y, a.z);
+                        d = mk(b.x, b.y, b.z);
+                        tmax = a.w;
+                        int pid = A.W.queue[A.bounce & 1][slot];
+                        L.pixel = __float_as_int(A.W.s2[pid].w);
+                        L.iter = __float_as_int(A.W.s3[pid].w);
+                    }
+                    T.start(L, o, d, tmax);
+                    active = true;
+                }
+            }
+        }
+        if (!__any_sync(FULL, active)) break;
+        while (active) {
+            T.step(L);
+            if (L.done) {
+                active = false;
+                if (ext) {
+                    uint32_t* h = A.ext_hits + size_t(item) * 5;
+                    if (MODE == 2) {
+                        h[0] = __float_as_uint(L.best.inst >= 0 ? 1.0f : -1.0f);
+                        h[1] = h[2] = 0xffffffffu;
+                        h[3] = h[4] = 0u;
+                    } else {
+                        h[0] = __float_as_uint(L.best.inst >= 0 ? L.best.t : -1.0f);
+                        h[1] = uint32_t(L.best.inst);
+                        h[2] = uint32_t(L.best.prim);
+                        h[3] = __float_as_uint(L.best.inst >= 0 ? L.best.u : 0.0f);
+                        h[4] = __float_as_uint(L.best.inst >= 0 ? L.best.v : 0.0f);
+                    }
+                } else if (MODE == 0) {
+                    bool hit = L.best.inst >= 0;
+                    A.W.hit[item] = make_float4(hit ? L.best.t : -1.0f, L.best.u, L.best.v, __int_as_float(L.best.inst));
+                    A.W.hit_prim[item] = L.best.prim;
+                    if (hit && A.nee) {
+                        // shadow ray of the raygen program (src/optixshaders/optix_triangle.cu:82-132)
+                        f3 n = hit_world_normal(A.S, L.best.inst, L.best.prim, L.best.u, L.best.v);
+                        f3 wo = L.world.o, wd = L.world.d;
+                        f3 hp = mk(__fadd_rn(wo.x, __fmul_rn(L.best.t, wd.x)), __fadd_rn(wo.y, __fmul_rn(L.best.t, wd.y)),
+                                   __fadd_rn(wo.z, __fmul_rn(L.best.t, wd.z)));
+                        f3 so = mk(__fadd_rn(hp.x, __fmul_rn(n.x, 1e-4f)), __fadd_rn(hp.y, __fmul_rn(n.y, 1e-4f)),
+                                   __fadd_rn(hp.z, __fmul_rn(n.z, 1e-4f)));
+                        int pid = A.W.queue[A.bounce & 1][item];
+                        float4 ns = A.W.s4[pid];
+                        f3 sd;
+                        float tmax;
+                        if (A.nee == 2) {
+                            sd = mk(ns.x, ns.y, ns.z);
+                            tmax = 1e16f;
+                        } else {
+                            f3 ld = mk(__fsub_rn(ns.x, so.x), __fsub_rn(ns.y, so.y), __fsub_rn(ns.z, so.z));
+                            float dl = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(ld.x, ld.x), __fmul_rn(ld.y, ld.y)), __fmul_rn(ld.z, ld.z)));
+                            float il = __fdiv_rn(1.0f, dl);
+                            sd = mk(__fmul_rn(ld.x, il), __fmul_rn(ld.y, il), __fmul_rn(ld.z, il));
+                            tmax = __fadd_rn(__fmul_rn(dl, 1.0001f), 1e-4f);
+                        }
+                        A.W.sh_o[item] = make_float4(so.x, so.y, so.z, tmax);
+                        A.W.sh_d[item] = make_float4(sd.x, sd.y, sd.z, 0.0f);
+                        // warp-aggregated append to the shadow queue
+                        unsigned am = __activemask();
+                        int leader = __ffs(am) - 1;
+                        int b2 = 0;
+                        if (lane == leader) b2 = atomicAdd(&A.W.ctr->shadow[A.bounce], __popc(am));
+                        b2 = __shfl_sync(am, b2, leader);
+                        A.W.sh_queue[b2 + __popc(am & ((1u << lane) - 1u))] = item;
+                    }
+                } else if (MODE == 1) {
+                    bool hit = L.best.inst >= 0;
+                    A.W.sh_hit[item] = make_float4(hit ? L.best.t : -1.0f, L.best.u, L.best.v, __int_as_float(L.best.inst));
+                    A.W.sh_prim[item] = L.best.prim;
+                } else {
+                    A.W.sh_hit[item] = make_float4(L.best.inst >= 0 ? 1.0f : -1.0f, 0.0f, 0.0f, __int_as_float(-1));
+                }
+                break;
+            }
+            if (__popc(__activemask()) < kRefill && !exhausted) break;
+        }
+    }
+}
+
+}  // namespace
+
+int trace_grid_blocks(int mode) {
+    static int cached[3] = {0, 0, 0};
+    if (cached[mode] == 0) {
+        int dev = 0, sms = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (mode == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace<0>, kTraceBlock, 0);
+        else if (mode == 1) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace<1>, kTraceBlock, 0);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace<2>, kTraceBlock, 0);
+        cached[mode] = sms * (per > 0 ? per : 1);
+    }
+    return cached[mode];
+}
+
+cudaError_t launch_trace(const DevScene& S, const DevWave& W, int bounce, int mode, int nee, cudaStream_t st) {
+    TraceArgs A{S, W, bounce, mode, nee, nullptr, nullptr, 0, 0, nullptr};
+    int grid = trace_grid_blocks(mode);
+    if (mode == 0) k_trace<0><<<grid, kTraceBlock, 0, st>>>(A);
+    else if (mode == 1) k_trace<1><<<grid, kTraceBlock, 0, st>>>(A);
+    else k_trace<2><<<grid, kTraceBlock, 0, st>>>(A);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_trace_ext(const DevScene& S, const DevWave& W, const float* rays, uint32_t* hits, int n, int mode,
+                             int iter, int* fetch, cudaStream_t st) {
+    TraceArgs A{S, W, 0, mode, 0, rays, hits, n, iter, fetch};
+    int grid = trace_grid_blocks(mode);
+    if (mode == 0) k_trace<0><<<grid, kTraceBlock, 0, st>>>(A);
+    else if (mode == 1) k_trace<1><<<grid, kTraceBlock, 0, st>>>(A);
+    else k_trace<2><<<grid, kTraceBlock, 0, st>>>(A);
+    return cudaGetLastError();
+}
+
+}  // namespace lux

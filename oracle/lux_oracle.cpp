@@ -155,13 +155,19 @@ template <class T> int select_from_cdf(const T* cdf, int size, T xi) {
 // ---------------------------------------------------------------------------------------
 // Textures. The reference uploads every texture as float4 (RGBA8 / 255, RGBA16 / 65535,
 // scene_load_gltf.cpp:115-143) into a cudaArray with linear filtering, wrap addressing and
-// normalised coordinates (src/texture.cu:51-56). The fetch below follows the public CUDA
-// programming guide's linear-filtering definition: xB = x*W - 0.5, i = floor(xB),
-// alpha = frac(xB) held with 8 fractional bits, tex = (1-a)(1-b)T[i,j] + a(1-b)T[i+1,j] +
-// (1-a)bT[i,j+1] + abT[i+1,j+1], indices wrapped.
+// normalised coordinates (src/texture.cu:51-56). The fetch below restates the CUDA hardware
+// filter as measured on B200 (tests/golden/texture_filter_probe.npz holds the measurement):
+// after wrap, x = u*W - 0.5, i = floor(x), the 1-D weight a = floor(frac(x)*256 + 0.5) in
+// 1/256 units (round half up; the programming guide's "9-bit fixed point with 8 fractional
+// bits"), likewise b; the 2-D weights are w00 = ((256-a)(256-b)+128)>>8, w11 = (ab+128)>>8,
+// w10 = (256-b) - w00, w01 = b - w11, summing to 256. Float texels are combined as
+// sum(w*T)/256; 8-bit unorm texels are expanded to 16 bits (c*257), combined in integers,
+// rounded half up to 16 bits and divided by 65535.
 struct Tex {
     int w = 0, h = 0;
-    std::vector<float> texels;  // w*h*4
+    bool unorm8 = false;         // texels kept as 8-bit unorm (hardware unorm path)
+    std::vector<float> texels;   // w*h*4 (float path)
+    std::vector<uint8_t> bytes;  // w*h*4 (unorm8 path)
 };
 
 inline float half_to_float(uint16_t h) {
@@ -185,10 +191,44 @@ inline float half_to_float(uint16_t h) {
     return f;
 }
 
-void load_tex(Tex& t, int w, int h, int fmt, const void* data) {
+inline float round_to_half(float f) {  // IEEE binary16 round-to-nearest-even, back to float
+    uint32_t x;
+    std::memcpy(&x, &f, 4);
+    uint32_t sign = (x >> 16) & 0x8000u;
+    int32_t e = int32_t((x >> 23) & 0xff) - 127 + 15;
+    uint32_t man = x & 0x7fffffu;
+    uint16_t hb;
+    if (((x >> 23) & 0xff) == 0xff) hb = uint16_t(sign | 0x7c00u | (man ? 0x200u : 0u));
+    else if (e >= 31) hb = uint16_t(sign | 0x7c00u);
+    else if (e <= 0) {
+        if (e < -10) hb = uint16_t(sign);
+        else {
+            man |= 0x800000u;
+            uint32_t shift = uint32_t(14 - e);
+            uint32_t half = man >> shift, rem = man & ((1u << shift) - 1u), mid = 1u << (shift - 1);
+            if (rem > mid || (rem == mid && (half & 1u))) ++half;
+            hb = uint16_t(sign | half);
+        }
+    } else {
+        uint32_t half = sign | (uint32_t(e) << 10) | (man >> 13), rem = man & 0x1fffu;
+        if (rem > 0x1000u || (rem == 0x1000u && (half & 1u))) ++half;
+        hb = uint16_t(half);
+    }
+    return half_to_float(hb);
+}
+
+// storage: LUX_TEXSTORE_FLOAT converts 8-bit texels to float as the reference does,
+// LUX_TEXSTORE_UNORM8 keeps them on the hardware unorm path, LUX_TEXSTORE_HALF rounds every
+// texel to binary16
+void load_tex(Tex& t, int w, int h, int fmt, const void* data, int storage = LUX_TEXSTORE_FLOAT) {
     t.w = w;
     t.h = h;
     size_t n = size_t(w) * size_t(h) * 4;
+    t.unorm8 = storage == LUX_TEXSTORE_UNORM8 && fmt == LUX_TEX_RGBA8;
+    if (t.unorm8) {
+        t.bytes.assign(static_cast<const uint8_t*>(data), static_cast<const uint8_t*>(data) + n);
+        return;
+    }
     t.texels.resize(n);
     for (size_t i = 0; i < n; ++i) {
         switch (fmt) {
@@ -197,6 +237,7 @@ void load_tex(Tex& t, int w, int h, int fmt, const void* data) {
             case LUX_TEX_RGBA16F: t.texels[i] = half_to_float(static_cast<const uint16_t*>(data)[i]); break;
             default: t.texels[i] = static_cast<const float*>(data)[i]; break;
         }
+        if (storage == LUX_TEXSTORE_HALF) t.texels[i] = round_to_half(t.texels[i]);
     }
 }
 
@@ -207,21 +248,30 @@ template <class T> void tex_fetch(const Tex& t, T u, T v, T out[4]) {
     float xb = uf * float(t.w) - 0.5f;
     float yb = vf * float(t.h) - 0.5f;
     float fi = std::floor(xb), fj = std::floor(yb);
-    float a = std::nearbyint((xb - fi) * 256.0f) * (1.0f / 256.0f);
-    float b = std::nearbyint((yb - fj) * 256.0f) * (1.0f / 256.0f);
+    int a = int(std::floor((xb - fi) * 256.0f + 0.5f));
+    int b = int(std::floor((yb - fj) * 256.0f + 0.5f));
+    int w00 = ((256 - a) * (256 - b) + 128) >> 8;
+    int w11 = (a * b + 128) >> 8;
+    int w10 = (256 - b) - w00;
+    int w01 = b - w11;
     int i0 = int(fi), j0 = int(fj);
     auto wrap = [](int i, int n) { int r = i % n; return r < 0 ? r + n : r; };
     int i1 = wrap(i0 + 1, t.w), j1 = wrap(j0 + 1, t.h);
     i0 = wrap(i0, t.w);
     j0 = wrap(j0, t.h);
-    const float* t00 = &t.texels[(size_t(j0) * t.w + i0) * 4];
-    const float* t10 = &t.texels[(size_t(j0) * t.w + i1) * 4];
-    const float* t01 = &t.texels[(size_t(j1) * t.w + i0) * 4];
-    const float* t11 = &t.texels[(size_t(j1) * t.w + i1) * 4];
+    size_t o00 = (size_t(j0) * t.w + i0) * 4, o10 = (size_t(j0) * t.w + i1) * 4;
+    size_t o01 = (size_t(j1) * t.w + i0) * 4, o11 = (size_t(j1) * t.w + i1) * 4;
     for (int c = 0; c < 4; ++c) {
-        float r = (1.0f - a) * (1.0f - b) * t00[c] + a * (1.0f - b) * t10[c] +
-                  (1.0f - a) * b * t01[c] + a * b * t11[c];
-        out[c] = T(r);
+        if (t.unorm8) {
+            int64_t s = int64_t(w00) * 257 * t.bytes[o00 + c] + int64_t(w10) * 257 * t.bytes[o10 + c] +
+                        int64_t(w01) * 257 * t.bytes[o01 + c] + int64_t(w11) * 257 * t.bytes[o11 + c];
+            int64_t r = (s + 128) >> 8;
+            out[c] = T(float(double(r) / 65535.0));
+        } else {
+            float r = (float(w00) * t.texels[o00 + c] + float(w10) * t.texels[o10 + c]) +
+                      (float(w01) * t.texels[o01 + c] + float(w11) * t.texels[o11 + c]);
+            out[c] = T(r * (1.0f / 256.0f));
+        }
     }
 }
 
@@ -1193,8 +1243,8 @@ bool shade_path(const orc_scene& s, const lux_options& opt, int iter, int depth,
                 else path.thr = path.thr / surv;
             }
         }
-        if (path.kill) return false;
-        // spawn the next ray (shade_path.cu:333-353, getPointOnRay include/intersections.h:29-32)
+        // spawn the next ray (shade_path.cu:333-353, getPointOnRay include/intersections.h:29-32);
+        // the reference runs it for paths killed above as well
         V3<T> hp = path.o + (is.t - T(.0001f)) * normalize(path.d);
         T sl2 = dot(sample_dir, sample_dir);
         if (!(sl2 > T(1e-12f)) || !std::isfinite(sl2)) {
@@ -1204,7 +1254,7 @@ bool shade_path(const orc_scene& s, const lux_options& opt, int iter, int depth,
         path.d = sample_dir;
         if (dot(path.d, is.normal) > T(0)) path.o = hp + (is.normal * T(kGLASS_EPS));
         else path.o = hp - (is.normal * T(kGLASS_EPS));
-        return compact;
+        return compact && !path.kill;
     }
     if (!path.kill && has_exr) {
         V3<T> d = normalize(path.d);
@@ -1438,7 +1488,7 @@ void orc_hemisphere(const float* normals, const int* seeds, int n, float* out) {
     }
 }
 
-orc_scene* orc_scene_create(const lux_scene_desc* d, int cdf_f64) {
+orc_scene* orc_scene_create(const lux_scene_desc* d, int cdf_f64, int tex_storage) {
     if (!d) return nullptr;
     orc_scene* s = new orc_scene();
     s->cam = d->camera;
@@ -1475,10 +1525,12 @@ orc_scene* orc_scene_create(const lux_scene_desc* d, int cdf_f64) {
     s->mats.assign(d->materials, d->materials + d->num_materials);
     s->texs.resize(d->num_textures);
     for (int i = 0; i < d->num_textures; ++i)
-        load_tex(s->texs[i], d->textures[i].width, d->textures[i].height, d->textures[i].format, d->textures[i].data);
+        load_tex(s->texs[i], d->textures[i].width, d->textures[i].height, d->textures[i].format, d->textures[i].data,
+                 tex_storage);
     if (d->env_data) {
         s->has_env = true;
-        load_tex(s->env, d->env_width, d->env_height, d->env_format, d->env_data);
+        load_tex(s->env, d->env_width, d->env_height, d->env_format, d->env_data,
+                 tex_storage == LUX_TEXSTORE_HALF ? LUX_TEXSTORE_HALF : LUX_TEXSTORE_FLOAT);
     }
     precompute_emissive<float>(*s, s->emissive_prefix, s->tri_prefix, s->total_area);
     precompute_emissive<double>(*s, s->emissive_prefix_d, s->tri_prefix_d, s->total_area_d);

@@ -35,8 +35,9 @@ void orc_sample_bsdf(const float* in, const int* seeds, int n, float* out);
 void orc_hemisphere(const float* normals, const int* seeds, int n, float* out);
 
 typedef struct orc_scene orc_scene;
-/* cdf_f64: 1 builds the light CDFs in FP64 (precision form), 0 in FP32 like the reference. */
-orc_scene* orc_scene_create(const lux_scene_desc* desc, int cdf_f64);
+/* cdf_f64: 1 builds the light CDFs in FP64 (precision form), 0 in FP32 like the reference.
+ * tex_storage: LUX_TEXSTORE_* of the CUDA path being checked. */
+orc_scene* orc_scene_create(const lux_scene_desc* desc, int cdf_f64, int tex_storage);
 void orc_scene_destroy(orc_scene* s);
 int orc_get_cdfs(orc_scene* s, float* emissive_prefix, float* tri_prefix, float* marginal,
                  float* conditional, float* total_area);
