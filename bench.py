@@ -1,0 +1,346 @@
+"""Benchmark of the render path on the 1M-triangle, 1920x1080, 16 spp, depth-12 workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step renders the whole job: 16 samples per pixel of the 1920x1080 frame of the seeded
+1M-triangle scene (200 instances of icospheres and displaced grids, random uber-shader
+materials, 16 value-noise 1024^2 textures, a 2048x1024 HDRI), trace depth 12, NEE with
+HDRI importance sampling (-dmis -emis). Rays are counted as traced: radiance plus shadow.
+
+Reported (one JSON line, rank 0):
+  value       Mrays/s of the device-timed render with the scene resident in HBM (all ranks)
+  e2e         the same metric through the C-ABI from host buffers: lux_init (scene upload,
+              BVH build, light tables), lux_render, lux_copy_image to host, lux_free
+  roofline    the traversal kernel (the dominant one): algorithmic bytes per launch over its
+              CUDA-event duration against the measured HBM copy bandwidth; the shading kernel
+              beside it
+  cpu_baseline  the reference's own render-path sources built for the host (oracle/_ref),
+              OpenMP over pixel rows, on a bounded crop of the same workload
+With --impl reference only that CPU arm runs (rank 0).
+Under torchrun every rank renders its own 16 samples (disjoint iterations, weak scaling) and
+the FP32 images are summed with one NCCL all-reduce per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mrays/s + served-job p50/p99 vs plain wavefront, 1 B200, equal relMSE"
+SPP = 16
+WORKLOAD = "1M tris / 200 instances, 1920x1080, 16 spp, depth 12, NEE + HDRI MIS (-dmis -emis), seed 0"
+# algorithmic bytes per path-bounce (fixed figures): trace I/O and shade
+TRACE_BYTES_PER_BOUNCE = 68.0  # radiance + shadow ray I/O of one path-bounce
+SHADE_BYTES_PER_BOUNCE = 244.0
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def make_scene():
+    import luxion_b200 as lx
+    return lx.random_scene(seed=0)
+
+
+class ClockSampler:
+    """nvidia-smi sampling during the timed region (every 200 ms)."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        try:
+            rows = [ln.split(",") for ln in open(self.path).read().strip().splitlines() if ln.strip()]
+            os.unlink(self.path)
+        except Exception:
+            return out
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+                for k, nm in enumerate(names):
+                    if r[5 + k].strip().lower() == "active":
+                        reasons.add(nm)
+            except Exception:
+                continue
+        if sm:
+            out["sm_mhz"] = float(np.median(sm))
+            out["sm_max_mhz"] = float(max(mx))
+            out["samples"] = len(sm)
+        out["reasons"] = sorted(reasons)
+        return out
+
+
+class CpuArm:
+    """The reference's own render-path sources built for the host (oracle/_ref; the oracle
+    port when that build is absent), OpenMP over pixel rows, on a centre crop of the frame."""
+
+    def __init__(self, scene, threads: int = 0):
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_lib as ol
+        from luxion_b200._ffi import default_options
+        self.opt = default_options(direct_light_sampling=1, env_importance_sampling=1)
+        self.kind = "reference" if ol.ref_available() else "port"
+        self.sc = ol.RefScene(scene) if self.kind == "reference" else ol.OracleScene(scene)
+        self.W, self.H = scene.width, scene.height
+        self.threads = threads or os.cpu_count()
+        self.side = 16
+
+    def run(self, it: int = 1):
+        x0, y0 = (self.W - self.side) // 2, (self.H - self.side) // 2
+        t0 = time.perf_counter()
+        _, st = self.sc.render(self.opt, it, 1, crop=(x0, y0, self.side, self.side), threads=self.threads)
+        return time.perf_counter() - t0, st
+
+    def calibrate(self, budget_s: float):
+        """Grow the crop until one run takes about budget_s."""
+        while True:
+            el, _ = self.run()
+            if el > budget_s / 4 or self.side * 2 > min(self.W, self.H):
+                break
+            self.side *= 2
+        return el
+
+    def measure(self, it: int = 1):
+        el, st = self.run(it)
+        rays = float(st[0] + st[1])
+        info = {"kind": self.kind, "cores": self.threads,
+                "sample": f"{self.side}x{self.side} centre crop of the 1920x1080 frame, 1 spp: {int(st[0])} radiance + "
+                          f"{int(st[1])} shadow rays in {el:.2f} s"}
+        return rays / el / 1e6, float(st[3]) / el, info
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    arm = CpuArm(make_scene())
+    arm.calibrate(8.0)
+    vals = []
+    info = None
+    for k in range(args.warmup + args.steps):
+        mr, sps, info = arm.measure(it=1 + k)
+        if k >= args.warmup:
+            vals.append(mr)
+    v = float(np.mean(vals))
+    line = {"metric": METRIC, "value": v, "unit": "Mrays/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+            "impl": "reference", "config": {"workload": WORKLOAD, "arm": "host build of the reference render path"},
+            "cpu_baseline": dict(info, value=v, unit="Mrays/s"),
+            "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    import luxion_b200 as lx
+    from luxion_b200._ffi import default_options
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    stream = torch.cuda.current_stream()
+    scene = make_scene()
+    opt = default_options(direct_light_sampling=1, env_importance_sampling=1, device=local,
+                          stream=stream.cuda_stream)
+    r = lx.Renderer(scene, opt)
+    W, H = scene.width, scene.height
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    img_dev = torch.zeros(W * H * 3, dtype=torch.float32, device="cuda") if world > 1 else None
+
+    def step(k):
+        r.reset()
+        r.render(1 + (rank * 1000 + k) * SPP, SPP)
+
+    for k in range(args.warmup):
+        step(k)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    rays = 0.0
+    launches = 0
+    ms = []
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        for k in range(args.steps):
+            flush.fill_(float(k))  # L2 flush between steps, outside the step's events
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step(args.warmup + k)
+            if world > 1:
+                # combine the ranks' sample sums (the one collective of the sharded path)
+                img = torch.from_numpy(r.image_sum().reshape(-1)).cuda()
+                dist.all_reduce(img)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+            st = r.stats()
+            rays += st["rays_radiance"] + st["rays_shadow"]
+            launches += int(st["kernel_launches"])
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+    clocks = clk.summary()
+    t_local = float(np.sum(ms))
+    if world > 1:
+        tt = torch.tensor([t_local, rays], dtype=torch.float64, device="cuda")
+        tmax = tt.clone()
+        dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(tt[1:], op=dist.ReduceOp.SUM)
+        t_all, rays_all = float(tmax[0]), float(tt[1])
+    else:
+        t_all, rays_all = t_local, rays
+    value = rays_all / (t_all * 1e-3) / 1e6
+    ms_per_step = t_all / args.steps
+
+    # per-kernel device times for the roofline (a separate timed pass: events around kernels)
+    r.enable_timing(True)
+    r.reset()
+    r.render(1, SPP)
+    kt = r.stats()
+    r.enable_timing(False)
+    hbm, peak_kind = peaks()
+    trace_bytes = TRACE_BYTES_PER_BOUNCE * kt["path_bounces"]
+    trace_ms_per_launch = kt["ms_trace"] / max(1.0, kt["launches_trace"])
+    trace_bytes_per_launch = trace_bytes / max(1.0, kt["launches_trace"])
+    ach = trace_bytes_per_launch / (trace_ms_per_launch * 1e-3) / 1e9
+    shade_bytes = SHADE_BYTES_PER_BOUNCE * kt["path_bounces"]
+    shade_ach = shade_bytes / (kt["ms_shade"] * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "trace_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get("bytes_per_launch_full_workload")
+    roof = {"bound": "hbm", "kernel": "k_trace (radiance + shadow)", "achieved": ach, "peak": hbm,
+            "unit": "GB/s", "frac": ach / hbm, "traffic": traffic, "peak_source": f"{peak_kind} MEASURED_PEAKS hbm_gbs",
+            "launch_ms": trace_ms_per_launch, "algorithmic_bytes_per_launch": trace_bytes_per_launch,
+            "note": "traversal is latency/L2 bound; BVH node and triangle reads are not counted as "
+                    "algorithmic bytes"}
+    roof_shade = {"bound": "hbm", "kernel": "k_shade", "achieved": shade_ach, "peak": hbm, "unit": "GB/s",
+                  "frac": shade_ach / hbm}
+    breakdown = {k: kt[k] for k in ("ms_total", "ms_trace", "ms_shade", "ms_camera", "ms_accum", "ms_sort")}
+
+    # end to end through the C-ABI from host buffers (cold: upload + build + render + readback)
+    e2e = None
+    if not args.no_e2e:
+        r.close()
+        e_ms, e_rays = [], 0.0
+        h2d = 0
+        img_host = np.empty((H, W, 3), np.float32)
+        for k in range(2):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            rr = lx.Renderer(scene, opt)
+            rr.render(1 + rank * SPP, SPP)
+            img_host[...] = rr.image_sum()
+            st = rr.stats()
+            rr.close()
+            torch.cuda.synchronize()
+            e_ms.append((time.perf_counter() - t0) * 1e3)
+            e_rays = st["rays_radiance"] + st["rays_shadow"]
+        d = scene.desc
+        for i in range(d.num_meshes):
+            m = d.meshes[i]
+            h2d += m.num_verts * (12 + (12 if m.normals else 0) + (8 if m.uvs else 0)) + m.num_tris * 12
+        for i in range(d.num_textures):
+            h2d += d.textures[i].width * d.textures[i].height * 4
+        h2d += d.env_width * d.env_height * 16 + d.num_instances * 208 + d.num_materials * 120
+        e2e = {"value": e_rays / (min(e_ms) * 1e-3) / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(W * H * 12), "ms_per_step": min(e_ms),
+               "includes": "lux_init (upload from pageable host memory, BVH8 build, light tables), "
+                           "lux_render 16 spp, lux_copy_image, lux_free"}
+    else:
+        r.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        arm = CpuArm(scene)
+        arm.calibrate(15.0)
+        mr, sps, info = arm.measure()
+        cpu = dict(info, value=mr, unit="Mrays/s", samples_per_s=sps)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {"metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene, random-init materials)",
+            "config": {"workload": WORKLOAD, "width": W, "height": H, "spp": SPP, "depth": 12,
+                       "instanced_tris": scene.instanced_tris, "form": "plain wavefront",
+                       "parallelism": f"spp-sharded x{world}" if world > 1 else "single GPU",
+                       "l2": "256 MiB buffer written between steps, outside the step events"},
+            "samples_per_s": (W * H * SPP * world) / (t_all * 1e-3),
+            "roofline": roof, "roofline_shade": roof_shade, "kernel_ms_one_step": breakdown,
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "gpu_launches": launches,
+            "served": None}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,339 @@
+"""Parity of the CUDA path (through the C-ABI) with the CPU oracle and with the golden vectors
+of the reference's own sources.
+
+Tolerances: integer and index outputs -- RNG streams, CDF tables and
+sample indices, hit instance/primitive ids, Morton keys, survivor sets -- bit-exact; hit
+distances and barycentrics bit-exact as well (the triangle test is evaluated with the same
+single-rounded operations); FP32 radiance within 1e-3 relative on >= 99.9% of pixels with
+image relMSE <= 1e-4.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import luxion_b200 as lx
+import oracle_lib as ol
+from luxion_b200 import _ffi
+from luxion_b200._ffi import default_options
+from luxion_b200.scene_builder import SceneBuilder
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden", "golden.npz")
+REL_TOL = 1e-3
+PIXEL_FRAC = 0.999
+RELMSE_TOL = 1e-4
+
+
+def bits(a):
+    return np.ascontiguousarray(a).view(np.uint32)
+
+
+@pytest.fixture(scope="module")
+def g():
+    return np.load(GOLD)
+
+
+def small_random_scene(**kw):
+    p = dict(seed=7, num_instances=8, total_tris=16000, min_tris=1000, max_tris=4000, num_emissive=2,
+             num_textures=4, texture_size=64, env_width=128, env_height=64, width=40, height=32, trace_depth=6)
+    p.update(kw)
+    return lx.random_scene(**p)
+
+
+OPTS = {"cornell": dict(direct_light_sampling=1), "rand": dict(direct_light_sampling=1, env_importance_sampling=1)}
+
+
+@pytest.fixture(scope="module", params=["cornell", "rand"])
+def pair(request):
+    tag = request.param
+    s = lx.cornell36(48, 48) if tag == "cornell" else small_random_scene()
+    r = lx.Renderer(s, default_options(**OPTS[tag]))
+    yield tag, s, r, ol.OracleScene(s), default_options(**OPTS[tag])
+    r.close()
+
+
+def image_parity(a, b):
+    rel = np.abs(a - b) / np.maximum(np.abs(b), 1e-6)
+    frac = float(np.mean(rel.max(axis=2) < REL_TOL))
+    relmse = float(np.mean((a - b) ** 2) / max(np.mean(b ** 2), 1e-30))
+    return frac, relmse
+
+
+# ---- integer streams --------------------------------------------------------------------------
+def test_rng_streams_bit_exact(g):
+    for (a, b, c), ref in zip(g["rng_seeds"], g["rng_streams"]):
+        assert np.array_equal(bits(lx.rng_stream(int(a), int(b), int(c), 32)), bits(ref))
+
+
+def test_cdfs_bit_exact(g, pair):
+    tag, s, r, o, _ = pair
+    cd = r.cdfs(o.cdf_sizes())
+    for k in ("emissive_prefix", "tri_prefix", "marginal", "conditional"):
+        assert np.array_equal(bits(cd[k]), bits(g[f"{tag}_cdf_{k}"])), k
+    assert np.float32(cd["total_area"]) == np.float32(g[f"{tag}_cdf_total_area"])
+
+
+def test_light_samples_bit_exact(g, pair):
+    tag, s, r, o, _ = pair
+    pix = np.arange(s.width * s.height, dtype=np.int32)
+    for depth in (0, 1, 4):
+        assert np.array_equal(bits(r.light_samples(pix, 3, depth)), bits(g[f"{tag}_light_d{depth}"])), depth
+
+
+def test_morton_keys_bit_exact(g, pair):
+    tag, s, r, o, _ = pair
+    assert np.array_equal(r.morton_keys(g[f"{tag}_rand_rays"]), g[f"{tag}_morton"])
+
+
+# ---- traversal ---------------------------------------------------------------------------------
+def test_trace_hits_bit_exact_golden(g, pair):
+    tag, s, r, o, _ = pair
+    rays = ol.camera_paths_to_rays(g[f"{tag}_camera_it3"])
+    assert np.array_equal(r.trace_rays(rays, 0, 3), g[f"{tag}_trace_cam"])
+    assert np.array_equal(r.trace_rays(g[f"{tag}_rand_rays"], 0, 3), g[f"{tag}_trace_rand_m0"])
+    assert np.array_equal(r.trace_rays(g[f"{tag}_rand_rays"], 2, 3)[:, 0], g[f"{tag}_trace_rand_m2"][:, 0])
+    assert np.array_equal(r.trace_rays(g[f"{tag}_rand_rays_tmax"], 1, 3), g[f"{tag}_trace_rand_m1"])
+
+
+@pytest.fixture(scope="module")
+def mid_scene():
+    s = lx.random_scene(seed=21, num_instances=40, total_tris=200000, min_tris=2000, max_tris=20000,
+                        num_emissive=4, num_textures=4, texture_size=64, env_width=64, env_height=32,
+                        width=64, height=36, trace_depth=8)
+    r = lx.Renderer(s, default_options(direct_light_sampling=1, env_importance_sampling=1))
+    yield s, r, ol.OracleScene(s)
+    r.close()
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_trace_hits_bit_exact_200k_tris(mid_scene, mode):
+    s, r, o = mid_scene
+    rays = ol.random_rays(200000, [-13, -0.5, -13], [13, 6, 13], seed=100 + mode)
+    if mode == 1:
+        rays[:, 3] = np.random.default_rng(1).uniform(0.01, 10.0, len(rays)).astype(np.float32)
+    hg, ho = r.trace_rays(rays, mode, 5), o.trace(rays, mode, 5)
+    if mode == 2:
+        hg, ho = hg[:, :1], ho[:, :1]
+    assert np.mean(hg[:, 0].view(np.float32) > 0) > 0.2
+    assert np.array_equal(hg, ho)
+
+
+def test_trace_edge_cases(mid_scene):
+    s, r, o = mid_scene
+    assert r.trace_rays(np.zeros((0, 8), np.float32), 0, 1).shape == (0, 5)
+    n = 4096
+    rng = np.random.default_rng(4)
+    rays = np.zeros((n, 8), np.float32)
+    rays[:, 0:3] = rng.uniform(-10, 10, (n, 3))
+    # axis-aligned directions (zero components -> infinite reciprocals) and huge origins
+    axes = np.eye(3, dtype=np.float32)[rng.integers(0, 3, n)] * rng.choice([-1.0, 1.0], (n, 1)).astype(np.float32)
+    rays[:, 4:7] = axes
+    rays[: n // 8, 0:3] *= 1e4
+    rays[:, 3] = 1e16
+    rays[:, 7] = np.arange(n, dtype=np.int32).view(np.float32)
+    for mode in (0, 2):
+        hg, ho = r.trace_rays(rays, mode, 1), o.trace(rays, mode, 1, brute=True)
+        if mode == 2:
+            hg, ho = hg[:, :1], ho[:, :1]
+        assert np.array_equal(hg, ho)
+    # rays pointing away from everything miss
+    away = ol.random_rays(1000, [100, 100, 100], [101, 101, 101], seed=3)
+    away[:, 4:7] = np.abs(away[:, 4:7])
+    assert np.all(r.trace_rays(away, 0, 1)[:, 0].view(np.float32) == -1.0)
+
+
+def test_alpha_mask_any_hit():
+    """A textured quad whose left half is cut out by the alpha mask (MASK) and one with BLEND."""
+    sb = SceneBuilder(16, 16)
+    tex = np.zeros((8, 8, 4), np.uint8)
+    tex[..., :3] = 200
+    tex[:, :4, 3] = 10      # transparent half (u < 0.5)
+    tex[:, 4:, 3] = 250
+    t = sb.add_texture(tex, _ffi.TEX_RGBA8)
+    quad = sb.add_mesh([[-1, -1, 0], [1, -1, 0], [1, 1, 0], [-1, 1, 0]], [[0, 1, 2], [0, 2, 3]],
+                       uvs=[[0, 0], [1, 0], [1, 1], [0, 1]])
+    m_mask = sb.add_material(albedo_tex=t, alpha_mode=_ffi.ALPHA_MASK, alpha_cutoff=0.5)
+    m_blend = sb.add_material(albedo_tex=t, alpha_mode=_ffi.ALPHA_BLEND, alpha=0.6)
+    sb.add_instance(quad, m_mask)
+    T = np.eye(4)
+    T[2, 3] = -1.0
+    sb.add_instance(quad, m_blend, T)
+    sb.set_env(np.ones((8, 16, 4), np.float32))
+    r = lx.Renderer(sb, default_options())
+    o = ol.OracleScene(sb)
+    n = 20000
+    rng = np.random.default_rng(0)
+    rays = np.zeros((n, 8), np.float32)
+    rays[:, 0] = rng.uniform(-1.2, 1.2, n)
+    rays[:, 1] = rng.uniform(-1.2, 1.2, n)
+    rays[:, 2] = 2.0
+    d = np.stack([rng.normal(0, 0.05, n), rng.normal(0, 0.05, n), -np.ones(n)], 1)
+    rays[:, 4:7] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    rays[:, 3] = 1e16
+    rays[:, 7] = np.arange(n, dtype=np.int32).view(np.float32)
+    for mode in (0, 2):
+        hg, ho = r.trace_rays(rays, mode, 3), o.trace(rays, mode, 3)
+        if mode == 2:
+            hg, ho = hg[:, :1], ho[:, :1]
+        assert np.array_equal(hg, ho)
+    hits = r.trace_rays(rays, 0, 3)
+    inst = hits[:, 1].astype(np.int64)
+    # every transparent-half ray passes the first quad
+    left = (rays[:, 0] < -0.1) & (np.abs(rays[:, 1]) < 0.9)
+    assert np.all(inst[left] != 0)
+    r.close()
+
+
+# ---- textures -----------------------------------------------------------------------------------
+@pytest.mark.parametrize("storage", [_ffi.TEXSTORE_FLOAT, _ffi.TEXSTORE_UNORM8, _ffi.TEXSTORE_HALF])
+def test_texture_filter_matches_hardware_model(storage):
+    sb = SceneBuilder(8, 8)
+    m = sb.add_mesh([[-1, -1, 0], [1, -1, 0], [1, 1, 0]], [[0, 1, 2]])
+    sb.add_instance(m, sb.add_material())
+    rng = np.random.default_rng(2)
+    t8 = sb.add_texture(rng.integers(0, 256, (37, 53, 4)).astype(np.uint8), _ffi.TEX_RGBA8)
+    tf = sb.add_texture(rng.uniform(0, 100, (16, 24, 4)).astype(np.float32), _ffi.TEX_RGBA32F)
+    oh = np.zeros((2, 2, 4), np.float32)
+    oh[0, 0, 3] = oh[0, 1, 0] = oh[1, 0, 1] = oh[1, 1, 2] = 1.0
+    t1 = sb.add_texture(oh, _ffi.TEX_RGBA32F)
+    sb.set_env(rng.uniform(0, 10, (32, 64, 4)).astype(np.float32))
+    r = lx.Renderer(sb, default_options(texture_storage=storage))
+    o = ol.OracleScene(sb, tex_storage=storage)
+    uv = rng.uniform(-3, 3, (20000, 2)).astype(np.float32)
+    for tex in (t8, tf, t1, -1):
+        a, b = r.sample_texture(tex, uv), o.sample_texture(tex, uv)
+        if tex == t1 or (tex == t8 and storage == _ffi.TEXSTORE_UNORM8):
+            assert np.array_equal(a, b), tex   # weights and unorm path are exact
+        else:
+            rel = np.abs(a - b) / np.maximum(np.abs(b), 1e-6)
+            assert rel.max() < 2e-6, (tex, rel.max())
+    r.close()
+
+
+# ---- shading -------------------------------------------------------------------------------------
+def test_shade_step_matches_reference(g, pair):
+    tag, s, r, o, opt = pair
+    paths, hits = g[f"{tag}_shade_in_paths"], g[f"{tag}_shade_in_hits"]
+    out, surv = r.shade_step(paths, hits, 3, 1, 1)
+    ref = g[f"{tag}_shade_out_paths"]
+    assert np.array_equal(np.sort(surv), g[f"{tag}_shade_survivors"])
+    live = ref[:, 19] == 0
+    for lo, hi in ((0, 3), (3, 6), (6, 9), (9, 12)):
+        a, b = out[:, lo:hi], ref[:, lo:hi]
+        rel = np.abs(a - b) / np.maximum(np.abs(b), 1e-6)
+        assert np.mean(rel.max(axis=1) < REL_TOL) >= PIXEL_FRAC, (lo, hi)
+    assert np.array_equal(out[:, 19], ref[:, 19])
+    assert np.array_equal(out[live, 20], ref[live, 20])
+
+
+# ---- end to end ---------------------------------------------------------------------------------
+def test_image_parity(pair):
+    tag, s, r, o, opt = pair
+    r.reset()
+    r.render(1, 16)
+    a = r.image_sum()
+    b, st = o.render(opt, 1, 16)
+    frac, relmse = image_parity(a, b)
+    assert frac >= PIXEL_FRAC and relmse <= RELMSE_TOL, (frac, relmse)
+    s_g = r.stats()
+    assert s_g["samples"] == 16 * s.width * s.height
+    assert s_g["rays_radiance"] == st[0] and s_g["rays_shadow"] == st[1]
+
+
+@pytest.mark.parametrize("dl,env", [(0, 0), (1, 0), (0, 1)])
+def test_image_parity_lighting_modes(dl, env):
+    s = small_random_scene(seed=9, width=32, height=24)
+    opt = default_options(direct_light_sampling=dl, env_importance_sampling=env)
+    r = lx.Renderer(s, opt)
+    r.render(1, 8)
+    frac, relmse = image_parity(r.image_sum(), ol.OracleScene(s).render(opt, 1, 8)[0])
+    r.close()
+    assert frac >= PIXEL_FRAC and relmse <= RELMSE_TOL, (frac, relmse)
+
+
+def test_batched_waves_graphs_and_sorting_give_identical_images():
+    s = small_random_scene(seed=11, width=48, height=40)
+    base = dict(direct_light_sampling=1, env_importance_sampling=1)
+    imgs = []
+    r = lx.Renderer(s, default_options(**base))
+    for it in range(1, 7):
+        r.render_iter(it)            # the reference's one-sample-per-call loop
+    imgs.append(r.image_sum())
+    r.close()
+    for kw in (dict(spp_per_wave=6), dict(spp_per_wave=4), dict(spp_per_wave=6, use_graph=0),
+               dict(spp_per_wave=5, ray_sorting=1)):
+        r = lx.Renderer(s, default_options(**base, **kw))
+        r.render(1, 6)
+        imgs.append(r.image_sum())
+        r.close()
+    for im in imgs[1:]:
+        assert np.array_equal(bits(im), bits(imgs[0]))
+
+
+def test_white_furnace():
+    """A smooth white metal sphere (F = 1, G ~ 1) under a constant environment of 1: every
+    pixel converges to 1 (energy conservation within 1e-3)."""
+    s = lx.furnace(48, 48, 24)
+    r = lx.Renderer(s, default_options(env_importance_sampling=1))
+    r.render(1, 32)
+    img = r.image_sum() / 32.0
+    r.close()
+    assert abs(float(img.mean()) - 1.0) < 1e-3
+    assert np.mean(np.abs(img - 1.0) < 1e-3) > 0.99
+
+
+def test_precision_form():
+    s = small_random_scene(seed=13, width=32, height=24)
+    opt_p = default_options(direct_light_sampling=1, env_importance_sampling=1)
+    opt_c = default_options(direct_light_sampling=1, env_importance_sampling=1,
+                            precision=_ffi.PRECISION_COMPENSATED, texture_storage=_ffi.TEXSTORE_HALF)
+    rp, rc = lx.Renderer(s, opt_p), lx.Renderer(s, opt_c)
+    o64 = ol.OracleScene(s, cdf_f64=1, tex_storage=_ffi.TEXSTORE_HALF)
+    cd = rc.cdfs(o64.cdf_sizes())
+    ref = o64.cdfs()
+    for k in ("emissive_prefix", "tri_prefix", "marginal", "conditional"):
+        assert np.array_equal(bits(cd[k]), bits(ref[k])), k
+    rp.render(1, 16)
+    rc.render(1, 16)
+    a, b = rp.image_sum(), rc.image_sum()
+    c = o64.render(opt_c, 1, 16)[0]
+    rp.close()
+    rc.close()
+    frac, relmse = image_parity(b, c)
+    assert relmse <= RELMSE_TOL, relmse
+    assert float(np.mean((a - b) ** 2) / np.mean(a ** 2)) < 0.05
+
+
+def test_reference_shaped_interface_and_pbo():
+    import torch
+    s = lx.cornell36(32, 32)
+    lx.PathTracerOptions.Get().direct_light_sampling = True
+    try:
+        lx.pathtraceInit(s)
+        pbo = torch.zeros(32 * 32 * 4, dtype=torch.uint8, device="cuda")
+        for it in range(1, 5):
+            lx.pathtrace(pbo.data_ptr(), 0, it)
+        img = lx.copyImageToHost()
+        rgba = pbo.cpu().numpy().reshape(32, 32, 4)
+    finally:
+        lx.pathtraceFree()
+        lx.PathTracerOptions.Get().direct_light_sampling = False
+    want = np.zeros((32 * 32, 4), np.uint8)
+    ol.orc().orc_tonemap(ol.f32p(np.ascontiguousarray(img)), 32 * 32, 4.0, 2,
+                         want.ctypes.data_as(__import__("ctypes").POINTER(__import__("ctypes").c_uint8)))
+    assert np.abs(rgba.reshape(-1, 4).astype(int) - want.astype(int)).max() <= 1
+
+
+def test_option_validation_on_device():
+    s = small_random_scene(env_width=0, env_height=0)
+    with pytest.raises(lx.LuxError) as e:
+        lx.Renderer(s, default_options(env_importance_sampling=1))
+    assert e.value.code == -1 and "environment" in str(e.value)
+    sb = SceneBuilder(8, 8)
+    m = sb.add_mesh([[-1, -1, 0], [1, -1, 0], [1, 1, 0]], [[0, 1, 2]])
+    sb.add_instance(m, sb.add_material())
+    with pytest.raises(lx.LuxError) as e:
+        lx.Renderer(sb, default_options(direct_light_sampling=1))
+    assert "emissive" in str(e.value)
