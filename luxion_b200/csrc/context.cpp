@@ -235,7 +235,9 @@ int make_texture(const lux_texture_desc& t, DevTex& out, int storage) {
 }
 
 // Texel values as the reference holds them (float4) for the HDRI CDF build.
-void env_texels(const lux_scene_desc& d, std::vector<float>& out) {
+// The environment texels the HDRI CDF is built from: the values the env texture holds on the
+// device, so that with binary16 storage the importance-sampling tables follow the stored map.
+void env_texels(const lux_scene_desc& d, int storage, std::vector<float>& out) {
     size_t n = size_t(d.env_width) * d.env_height * 4;
     out.resize(n);
     if (d.env_format == LUX_TEX_RGBA16F) {
@@ -244,6 +246,8 @@ void env_texels(const lux_scene_desc& d, std::vector<float>& out) {
     } else {
         const float* s = static_cast<const float*>(d.env_data);
         std::copy(s, s + n, out.begin());
+        if (storage == LUX_TEXSTORE_HALF)
+            for (size_t i = 0; i < n; ++i) out[i] = __half2float(__float2half_rn(out[i]));
     }
 }
 
@@ -550,7 +554,7 @@ int build_scene(lux_ctx* C, const lux_scene_desc& d) {
     }
     // ---- light tables ----
     std::vector<float> envt;
-    if (d.env_data) env_texels(d, envt);
+    if (d.env_data) env_texels(d, C->opt.texture_storage, envt);
     std::vector<int> emissive;
     std::vector<std::vector<float>> tri_prefix;
     bool env_ok;

