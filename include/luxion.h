@@ -233,6 +233,26 @@ int lux_get_stats(lux_ctx* ctx, lux_stats* out);
  * mode 2 only word 0 is meaningful (1.0 occluded, -1.0 free). Host buffers. */
 int lux_trace_rays(lux_ctx* ctx, const float* rays, int n, int mode, int iter, uint32_t* hits);
 
+/* lux_trace_rays_static: lux_trace_rays for callers that must not allocate device memory on
+ * the call. No counterpart in the reference. Same arguments, results and errors as
+ * lux_trace_rays, for n <= LUX_TRACE_STATIC_MAX_RAYS; a larger n is rejected with
+ * LUX_ERR_INVALID before any device work.
+ * Who needs it: a host that has given the device's free memory to its own pool or to other
+ * tenants under a fixed budget, where a per-call cudaMalloc can fail in the middle of a
+ * request; and a host that keeps other work running on other streams of the device, which
+ * the per-call cudaFree of lux_trace_rays stalls (cudaFree waits for the whole device).
+ * Rays and hits are staged through one fixed array of 256 + 52 * LUX_TRACE_STATIC_MAX_RAYS
+ * bytes (about 3.25 MiB) compiled into the library, one copy per device. Its address is
+ * looked up (cudaGetSymbolAddress) on the first call made on each device, so make that first
+ * call before any stream capture begins on that device.
+ * Must start at zero: the traversal's work cursor in that array and the context's traversal
+ * error word; the call clears both on the context's stream before its launch. Nothing else
+ * carries over from one call to the next.
+ * Calls that overlap on one device (two threads, or two contexts on the same device) share
+ * the array and race: the library does not lock it, so serialise such calls. */
+#define LUX_TRACE_STATIC_MAX_RAYS 65536
+int lux_trace_rays_static(lux_ctx* ctx, const float* rays, int n, int mode, int iter, uint32_t* hits);
+
 /* Morton keys of caller rays (src/morton_codes.cu:13-24, src/kernels/intersection_precompute.cu:6-33):
  * rays as in lux_trace_rays; keys: n u32. Host buffers. */
 int lux_morton_keys(lux_ctx* ctx, const float* rays, int n, uint32_t* keys);

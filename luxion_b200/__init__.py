@@ -45,6 +45,7 @@ SIGNATURES = {
     "lux_enable_timing": (C.c_int, [_P, C.c_int]),
     "lux_get_stats": (C.c_int, [_P, C.POINTER(Stats)]),
     "lux_trace_rays": (C.c_int, [_P, c_float_p, C.c_int, C.c_int, C.c_int, c_u32_p]),
+    "lux_trace_rays_static": (C.c_int, [_P, c_float_p, C.c_int, C.c_int, C.c_int, c_u32_p]),
     "lux_morton_keys": (C.c_int, [_P, c_float_p, C.c_int, c_u32_p]),
     "lux_shade_step": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, c_float_p, C.c_int, c_u32_p, c_int_p, c_int_p]),
     "lux_light_samples": (C.c_int, [_P, C.c_int, C.c_int, c_int_p, C.c_int, c_float_p]),
@@ -201,6 +202,15 @@ class Renderer:
         n = rays.shape[0]
         hits = np.zeros((n, 5), np.uint32)
         _check(lib().lux_trace_rays(self._h, ptr(rays), n, mode, it, ptr(hits, C.c_uint32)))
+        return hits
+
+    def trace_rays_static(self, rays: np.ndarray, mode: int = 0, it: int = 1) -> np.ndarray:
+        """trace_rays through the library's fixed device scratch (no device allocation on the
+        call), for at most TRACE_STATIC_MAX_RAYS rays; overlapping calls on one device race."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = rays.shape[0]
+        hits = np.zeros((n, 5), np.uint32)
+        _check(lib().lux_trace_rays_static(self._h, ptr(rays), n, mode, it, ptr(hits, C.c_uint32)))
         return hits
 
     def morton_keys(self, rays: np.ndarray) -> np.ndarray:

@@ -28,6 +28,7 @@ ALPHA_OPAQUE, ALPHA_MASK, ALPHA_BLEND = 0, 1, 2
 TONEMAP_REINHARD, TONEMAP_AGX, TONEMAP_ACES = 0, 1, 2
 PRECISION_PLAIN, PRECISION_COMPENSATED = 0, 1
 TEXSTORE_FLOAT, TEXSTORE_UNORM8, TEXSTORE_HALF = 0, 1, 2
+TRACE_STATIC_MAX_RAYS = 65536  # LUX_TRACE_STATIC_MAX_RAYS
 
 # path-state layout (LUX_PS_*)
 PS_ORIGIN, PS_DIR, PS_COLOR, PS_THROUGHPUT = 0, 3, 6, 9

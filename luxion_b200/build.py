@@ -8,6 +8,7 @@ Translation units:
   shade.cu    camera / shade / accumulate kernels, --fmad=false so every float op is
               rounded on its own, in the reference's order
   sort.cu     Morton keys and the radix sort of a bounce queue
+  trace_static.cu  the fixed device scratch of lux_trace_rays_static
   context.cpp, bvh_build.cpp, scene_gen.cpp   host C++ (no FMA contraction)
 The CUDA runtime is linked statically so the library does not depend on which libcudart a
 host process (for example PyTorch) has already loaded.
@@ -34,6 +35,7 @@ CU_UNITS = {
     "trace.cu": ["--fmad=true"],
     "shade.cu": ["--fmad=false"],
     "sort.cu": ["--fmad=true"],
+    "trace_static.cu": ["--fmad=true"],
 }
 CPP_UNITS = ["context.cpp", "bvh_build.cpp", "scene_gen.cpp"]
 

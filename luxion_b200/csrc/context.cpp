@@ -1058,6 +1058,31 @@ int lux_trace_rays(lux_ctx* C, const float* rays, int n, int mode, int iter, uin
     return LUX_OK;
 }
 
+int lux_trace_rays_static(lux_ctx* C, const float* rays, int n, int mode, int iter, uint32_t* hits) {
+    if (!C || (!rays && n > 0) || (!hits && n > 0) || n < 0 || mode < 0 || mode > 2)
+        return fail(LUX_ERR_INVALID, "bad arguments");
+    if (n > LUX_TRACE_STATIC_MAX_RAYS)
+        return fail(LUX_ERR_INVALID, "lux_trace_rays_static: n = " + std::to_string(n) +
+                                         " exceeds LUX_TRACE_STATIC_MAX_RAYS (" +
+                                         std::to_string(LUX_TRACE_STATIC_MAX_RAYS) +
+                                         "); split the batch or call lux_trace_rays");
+    if (n == 0) return LUX_OK;
+    LUX_CUDA(cudaSetDevice(C->device));
+    TraceScratch sc;
+    LUX_CUDA(trace_static_scratch(C->device, sc));
+    LUX_CUDA(cudaMemcpyAsync(sc.rays, rays, size_t(n) * 8 * sizeof(float), cudaMemcpyHostToDevice, C->stream));
+    // the work cursor and the traversal error word must start at zero
+    LUX_CUDA(cudaMemsetAsync(sc.cursor, 0, sizeof(int), C->stream));
+    LUX_CUDA(cudaMemsetAsync(C->W.ctr, 0, sizeof(WaveCounters), C->stream));
+    LUX_CUDA(launch_trace_ext(C->S, C->W, sc.rays, sc.hits, n, mode, iter, sc.cursor, C->stream));
+    LUX_CUDA(cudaMemcpyAsync(hits, sc.hits, size_t(n) * 5 * sizeof(uint32_t), cudaMemcpyDeviceToHost, C->stream));
+    WaveCounters hc;
+    LUX_CUDA(cudaMemcpyAsync(&hc, C->W.ctr, sizeof(hc), cudaMemcpyDeviceToHost, C->stream));
+    LUX_CUDA(cudaStreamSynchronize(C->stream));
+    if (hc.error) return fail(LUX_ERR_UNSUPPORTED, "traversal stack overflow");
+    return LUX_OK;
+}
+
 int lux_morton_keys(lux_ctx* C, const float* rays, int n, uint32_t* keys) {
     if (!C || n < 0 || (n > 0 && (!rays || !keys))) return fail(LUX_ERR_INVALID, "bad arguments");
     if (n == 0) return LUX_OK;

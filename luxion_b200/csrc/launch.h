@@ -19,6 +19,16 @@ cudaError_t launch_trace(const DevScene& S, const DevWave& W, int bounce, int mo
 cudaError_t launch_trace_ext(const DevScene& S, const DevWave& W, const float* rays, uint32_t* hits, int n, int mode,
                              int iter, int* fetch, cudaStream_t st);
 
+// the fixed scratch of lux_trace_rays_static on `device` (trace_static.cu), which must be the
+// current device on the first call for it: cursor, then LUX_TRACE_STATIC_MAX_RAYS rays and hits
+struct TraceScratch {
+    int* cursor;
+    float* rays;
+    uint32_t* hits;
+};
+cudaError_t trace_static_scratch(int device, TraceScratch& out);
+size_t trace_static_scratch_bytes();
+
 // camera rays for paths [0, n) of the wave (+ NEE sample of bounce 0), queue 0 = identity
 cudaError_t launch_camera(const DevScene& S, const DevWave& W, const DevOptions& O, const DevCamera& cam, int n,
                           cudaStream_t st);

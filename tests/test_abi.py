@@ -130,3 +130,9 @@ def test_procedural_scenes():
     assert np.array_equal(a, b)
     f = lx.furnace(16, 16, 4)
     assert f.desc.env_data is not None and f.desc.num_instances == 1
+
+
+def test_static_trace_limit_matches_header():
+    text = open(HEADER).read()
+    m = re.search(r"#define LUX_TRACE_STATIC_MAX_RAYS (\d+)", text)
+    assert m and int(m.group(1)) == _ffi.TRACE_STATIC_MAX_RAYS
