@@ -165,7 +165,8 @@ float half_bits_to_float(uint16_t h) {
 
 // Upload one texture. storage LUX_TEXSTORE_FLOAT converts 8/16-bit unorm texels to float4 as
 // TextureHandler::load_textures_on_device does (c/255, c/65535; src/texture.cu:12-69),
-// LUX_TEXSTORE_HALF converts them to binary16, LUX_TEXSTORE_UNORM8 keeps 8-bit texels.
+// LUX_TEXSTORE_HALF converts them to binary16, LUX_TEXSTORE_UNORM8 keeps 8-bit texels (16-bit
+// ones become float4). Binary16 texels stay binary16 under every storage.
 int make_texture(const lux_texture_desc& t, DevTex& out, int storage) {
     if (t.width <= 0 || t.height <= 0 || !t.data) return fail(LUX_ERR_INVALID, "empty texture");
     const size_t n = size_t(t.width) * t.height * 4;
@@ -186,7 +187,8 @@ int make_texture(const lux_texture_desc& t, DevTex& out, int storage) {
         for (size_t i = 0; i < n; ++i) f16[i] = __float2half_rn(to_float(i));
         src = f16.data();
         fmt = LUX_TEX_RGBA16F;
-    } else if (storage == LUX_TEXSTORE_FLOAT && (t.format == LUX_TEX_RGBA8 || t.format == LUX_TEX_RGBA16)) {
+    } else if ((storage == LUX_TEXSTORE_FLOAT && t.format == LUX_TEX_RGBA8) ||
+               (storage != LUX_TEXSTORE_HALF && t.format == LUX_TEX_RGBA16)) {
         f32.resize(n);
         for (size_t i = 0; i < n; ++i) f32[i] = to_float(i);
         src = f32.data();

@@ -5,7 +5,7 @@
 Textures whose texel (i, j) holds 1 in channel (i % 2) + 2 * (j % 2) and 0 elsewhere make
 every fetch return its four 2-D filter weights, one per channel. The script samples them at
 random and at grid coordinates on textures of several sizes, plus an 8-bit ramp for the
-unorm path, and stores every fourth sample, with the weights as integers in units of 1/256,
+unorm path and random texels stored as binary16, and stores every fourth sample, with the weights as integers in units of 1/256,
 in texture_filter_probe.npz. The oracle's texture fetch (oracle/lux_oracle.cpp, tex_axis and
 tex_fetch) restates the rule these data pin, and tests/test_texture_model.py checks it against
 them on the CPU. `--compact-from RAW.npz` rewrites a full-size measurement (PROBE_RAW=1 keeps
@@ -59,6 +59,23 @@ def main():
     out["ramp"] = ramp
     out["v_ramp"] = r.sample_texture(t_ramp, uv)
     r.close()
+    # binary16 storage: random texels (uniform, 8-bit, and over six decades) filtered from half
+    sb = SceneBuilder(8, 8)
+    m = sb.add_mesh([[-1, -1, 0], [1, -1, 0], [1, 1, 0]], [[0, 1, 2]])
+    sb.add_instance(m, sb.add_material())
+    half_src = [rng.uniform(0, 100, (16, 24, 4)).astype(np.float32),
+                rng.integers(0, 256, (37, 53, 4)).astype(np.uint8),
+                np.exp(rng.uniform(np.log(1e-3), np.log(1e3), (32, 64, 4))).astype(np.float32)]
+    hids = [sb.add_texture(t, _ffi.TEX_RGBA8 if t.dtype == np.uint8 else _ffi.TEX_RGBA32F) for t in half_src]
+    sb.set_env(np.ones((4, 8, 4), np.float32))
+    r = lx.Renderer(sb, lx.default_options(texture_storage=_ffi.TEXSTORE_HALF))
+    for k, (t, tid) in enumerate(zip(half_src, hids)):
+        f = t.astype(np.float32) / np.float32(255) if t.dtype == np.uint8 else t
+        out[f"half_tex_{k}"] = f.astype(np.float16)
+        uv = rng.uniform(-3, 3, (6000, 2)).astype(np.float32)
+        out[f"half_uv_{k}"] = uv
+        out[f"half_v_{k}"] = r.sample_texture(tid, uv)
+    r.close()
     dst = os.environ.get("PROBE_OUT", os.path.join(HERE, "texture_filter_probe.npz"))
     np.savez_compressed(dst, **(out if os.environ.get("PROBE_RAW") else compact(out)))
     print("wrote", dst)
@@ -74,6 +91,10 @@ def compact(raw):
         out[f"w_{k}"] = w.astype(np.uint16)
     out["uv_ramp"] = raw["uv_ramp"][::4]
     out["v_ramp"] = raw["v_ramp"][::4]
+    for k in ("half_tex", "half_uv", "half_v"):
+        for i in range(3):
+            if f"{k}_{i}" in raw:
+                out[f"{k}_{i}"] = raw[f"{k}_{i}"]
     return out
 
 

@@ -64,3 +64,33 @@ def test_a_plain_float_product_model_would_not_match():
     i0 = np.floor(x).astype(np.int64) % 2
     a_meas = np.where(i0 == 0, wt[:, 1] + wt[:, 3], wt[:, 0] + wt[:, 2])
     assert (a_meas != a_fp32).sum() > 50
+
+
+def test_binary16_filter_matches_hardware():
+    """Texels held as binary16 (the precision form's storage, and any RGBA16F input) take the
+    hardware's half filter: block-aligned 15-bit texels, exact sum, ties away from zero."""
+    sb = SceneBuilder(8, 8)
+    m = sb.add_mesh([[-1, -1, 0], [1, -1, 0], [1, 1, 0]], [[0, 1, 2]])
+    sb.add_instance(m, sb.add_material())
+    ids = [sb.add_texture(PROBE[f"half_tex_{k}"], _ffi.TEX_RGBA16F) for k in range(3)]
+    sb.set_env(np.ones((4, 8, 4), np.float32))
+    o = ol.OracleScene(sb, tex_storage=_ffi.TEXSTORE_FLOAT)
+    for k, tex in enumerate(ids):
+        got = o.sample_texture(tex, PROBE[f"half_uv_{k}"])
+        want = PROBE[f"half_v_{k}"]
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), (k, int((got != want).sum()))
+
+
+def test_binary16_storage_rounds_then_filters_as_half():
+    """Float input under LUX_TEXSTORE_HALF: texels round to nearest-even binary16 first."""
+    tex = PROBE["half_tex_0"]
+    sb = SceneBuilder(8, 8)
+    m = sb.add_mesh([[-1, -1, 0], [1, -1, 0], [1, 1, 0]], [[0, 1, 2]])
+    sb.add_instance(m, sb.add_material())
+    t_half = sb.add_texture(tex, _ffi.TEX_RGBA16F)
+    # the same texels given as float32 with a residue below half precision
+    t_f32 = sb.add_texture(tex.astype(np.float32) * np.float32(1 + 2 ** -13), _ffi.TEX_RGBA32F)
+    sb.set_env(np.ones((4, 8, 4), np.float32))
+    o = ol.OracleScene(sb, tex_storage=_ffi.TEXSTORE_HALF)
+    uv = PROBE["half_uv_0"]
+    assert np.array_equal(o.sample_texture(t_half, uv), o.sample_texture(t_f32, uv))
