@@ -38,8 +38,13 @@ constexpr int kLocStack = 48;
 constexpr int kRefill = 20;
 constexpr uint32_t kTagMask = 3u << 30;
 constexpr uint32_t kTagNode = 0u;
+constexpr uint32_t kTagTri = 1u << 30;
 constexpr uint32_t kTagInst = 2u << 30;
 constexpr uint32_t kTagMarker = 3u << 30;
+constexpr uint32_t kRecMask = 0xffffffu;
+// fewer lanes than this with triangles to test: push the triangle groups and keep
+// traversing nodes (the postponement of Ylitie et al. 2017)
+constexpr int kPostpone = 8;
 constexpr float kLo = 1.0f - 1.0f / 524288.0f;
 constexpr float kHi = 1.0f + 1.0f / 524288.0f;
 
@@ -182,12 +187,15 @@ LUX_DI bool alpha_accept(const DevScene& S, const DevInstance& I, int inst, int 
     return !(rnd >= alpha);
 }
 
-// Traversal state of one lane.
+// Traversal state of one lane. The world ray is kept as origin and direction only; its
+// reciprocals are recomputed when the traversal leaves an instance.
 struct Lane {
-    TRay world, cur;
+    f3 wo, wd;          // world ray
+    TRay cur;           // ray of the current level (world in the TLAS, object space in a BLAS)
     float tmax;
     Best best;
-    uint2 grp;          // current group
+    uint2 g;            // node group: x = first internal child, y = imask << 8 | remaining hit keys
+    uint2 t;            // leaf group: x = first record, y = tag (kTagTri / kTagInst) | record mask
     int sp;             // stack depth
     int inst;           // current instance (-1 in the TLAS)
     int inst_flags;
@@ -219,8 +227,9 @@ struct Tracer {
     }
 
     LUX_DI void start(Lane& L, f3 o, f3 d, float tmax) {
-        L.world = make_ray(o, d);
-        L.cur = L.world;
+        L.wo = o;
+        L.wd = d;
+        L.cur = make_ray(o, d);
         L.tmax = tmax;
         L.best.t = -1.0f;
         L.best.inst = -1;
@@ -229,99 +238,91 @@ struct Tracer {
         L.sp = 0;
         L.inst = -1;
         L.inst_flags = 0;
+        L.inst_prim_base = 0;
         L.done = false;
-        // root group: a single internal "child" = the TLAS root, at key oct (slot 0)
-        L.grp = make_uint2(S.tlas_root, kTagNode | (1u << 8) | (1u << L.cur.oct));
+        // root group: a single internal child (slot 0) = the TLAS root, at key oct
+        L.g = make_uint2(S.tlas_root, (1u << 8) | (1u << L.cur.oct));
+        L.t = make_uint2(0u, 0u);
     }
 
     LUX_DI float limit(const Lane& L) const { return (MODE != 2 && L.best.inst >= 0) ? L.best.t : L.tmax; }
 
-    LUX_DI void enter_instance(Lane& L, int ii) {
-        const DevInstance& I = S.insts[ii];
-        f3 oo = xform(I.Minv, L.world.o, 1.0f);
-        f3 od = xform(I.Minv, L.world.d, 0.0f);
+    // Node phase: visit the nearest remaining child of the node group.
+    LUX_DI void visit(Lane& L) {
+        uint32_t keys = L.g.y & 0xffu;
+        uint32_t key = __ffs(keys) - 1;
+        keys &= keys - 1;
+        uint32_t slot = key ^ L.cur.oct;
+        uint32_t imask = L.g.y >> 8;
+        uint32_t child = L.g.x + __popc(imask & ((1u << slot) - 1u));
+        if (keys) push(L, make_uint2(L.g.x, (imask << 8) | keys));
+        uint32_t nkeys, nimask, cbase, tbase, tmask;
+        visit_node(S.nodes, child, L.cur, limit(L), nkeys, nimask, cbase, tbase, tmask);
+        L.g = make_uint2(cbase, (nimask << 8) | nkeys);
+        if (tmask) {
+            if (L.inst >= 0) L.t = make_uint2(L.inst_prim_base + tbase, kTagTri | tmask);
+            else L.t = make_uint2(tbase, kTagInst | tmask);
+        }
+    }
+
+    // Triangle phase: test the lowest triangle of the leaf group.
+    LUX_DI void test_one(Lane& L) {
+        uint32_t m = L.t.y & kRecMask;
+        int k = __ffs(m) - 1;
+        m &= m - 1;
+        L.t.y = m ? (kTagTri | m) : 0u;
+        float t, u, v;
+        int prim;
+        if (!mt_test(S.prims, L.t.x + uint32_t(k), L.cur, t, u, v, prim)) return;
+        if (!(t <= L.tmax)) return;
+        if (MODE != 2 && !better(t, L.inst, prim, L.best)) return;
+        if (L.inst_flags & kInstAnyHit) {
+            if (!alpha_accept(S, S.insts[L.inst], L.inst, prim, u, v, L.wd, L.pixel, L.iter)) return;
+        }
+        L.best.t = t;
+        L.best.inst = L.inst;
+        L.best.prim = prim;
+        L.best.u = u;
+        L.best.v = v;
+        if (MODE == 2) L.done = true;
+    }
+
+    // Instance phase: enter the lowest instance of a TLAS leaf group. The world-level node
+    // group and the rest of the leaf group wait on the stack under a marker.
+    LUX_DI void enter(Lane& L) {
+        uint32_t m = L.t.y & kRecMask;
+        int k = __ffs(m) - 1;
+        m &= m - 1;
+        int ii = int(__ldg(S.tlas_prims + L.t.x + uint32_t(k)));
+        if (L.g.y & 0xffu) push(L, L.g);
+        if (m) push(L, make_uint2(L.t.x, kTagInst | m));
         push(L, make_uint2(0u, kTagMarker));
-        L.cur = make_ray(oo, od);
+        const DevInstance& I = S.insts[ii];
+        L.cur = make_ray(xform(I.Minv, L.wo, 1.0f), xform(I.Minv, L.wd, 0.0f));
         L.inst = ii;
         L.inst_flags = I.flags;
         L.inst_prim_base = I.prim_base;
-        L.grp = make_uint2(I.blas_root, kTagNode | (1u << 8) | (1u << L.cur.oct));
+        L.g = make_uint2(I.blas_root, (1u << 8) | (1u << L.cur.oct));
+        L.t = make_uint2(0u, 0u);
     }
 
-    LUX_DI void test_prims(Lane& L, uint32_t base, uint32_t mask) {
-        while (mask) {
-            int k = __ffs(mask) - 1;
-            mask &= mask - 1;
-            float t, u, v;
-            int prim;
-            if (!mt_test(S.prims, L.inst_prim_base + base + uint32_t(k), L.cur, t, u, v, prim)) continue;
-            if (!(t <= L.tmax)) continue;
-            if (MODE != 2 && !better(t, L.inst, prim, L.best)) continue;
-            if (L.inst_flags & kInstAnyHit) {
-                if (!alpha_accept(S, S.insts[L.inst], L.inst, prim, u, v, L.world.d, L.pixel, L.iter)) continue;
-            }
-            L.best.t = t;
-            L.best.inst = L.inst;
-            L.best.prim = prim;
-            L.best.u = u;
-            L.best.v = v;
-            if (MODE == 2) {
-                L.done = true;
-                return;
-            }
-        }
-    }
-
-    // One traversal step; sets L.done when the ray is finished.
-    LUX_DI void step(Lane& L) {
-        uint32_t tag = L.grp.y & kTagMask;
-        if (tag == kTagNode && (L.grp.y & 0xffu)) {
-            uint32_t keys = L.grp.y & 0xffu;
-            uint32_t key = __ffs(keys) - 1;
-            keys &= keys - 1;
-            uint32_t slot = key ^ L.cur.oct;
-            uint32_t imask = (L.grp.y >> 8) & 0xffu;
-            uint32_t child = L.grp.x + __popc(imask & ((1u << slot) - 1u));
-            if (keys) push(L, make_uint2(L.grp.x, (L.grp.y & ~0xffu) | keys));
-            uint32_t nkeys, nimask, cbase, tbase, tmask;
-            visit_node(S.nodes, child, L.cur, limit(L), nkeys, nimask, cbase, tbase, tmask);
-            if (tmask) {
-                if (L.inst >= 0) {
-                    test_prims(L, tbase, tmask);
-                    if (L.done) return;
-                } else {
-                    // TLAS leaves: instances, handled as a group after the node group
-                    if (nkeys) push(L, make_uint2(cbase, kTagNode | (nimask << 8) | nkeys));
-                    L.grp = make_uint2(tbase, kTagInst | tmask);
-                    return;
-                }
-            }
-            L.grp = make_uint2(cbase, kTagNode | (nimask << 8) | nkeys);
-            return;
-        }
-        if (tag == kTagInst && (L.grp.y & 0xffffffu)) {
-            uint32_t m = L.grp.y & 0xffffffu;
-            int k = __ffs(m) - 1;
-            m &= m - 1;
-            int ii = int(__ldg(S.tlas_prims + L.grp.x + uint32_t(k)));
-            if (m) push(L, make_uint2(L.grp.x, kTagInst | m));
-            enter_instance(L, ii);
-            return;
-        }
-        // current group exhausted: pop
+    // Pop phase: take the next group from the stack; the ray is done when it is empty.
+    LUX_DI void next(Lane& L) {
         while (true) {
             if (L.sp == 0) {
                 L.done = true;
                 return;
             }
             uint2 e = pop(L);
-            if ((e.y & kTagMask) == kTagMarker) {
-                L.cur = L.world;
+            uint32_t tag = e.y & kTagMask;
+            if (tag == kTagMarker) {
+                L.cur = make_ray(L.wo, L.wd);
                 L.inst = -1;
                 L.inst_flags = 0;
                 continue;
             }
-            L.grp = e;
+            if (tag == kTagNode) L.g = e;
+            else L.t = e;
             return;
         }
     }
@@ -374,7 +375,7 @@ LUX_DI f3 hit_world_normal(const DevScene& S, int inst, int prim, float bu, floa
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kTraceBlock, 4) k_trace(TraceArgs A) {
+__global__ void __launch_bounds__(kTraceBlock, 6) k_trace(TraceArgs A) {
     __shared__ uint2 stack[kShStack][kTraceBlock];
     Tracer<MODE> T{A.S, stack, {}, int(threadIdx.x), &A.W.ctr->error};
     const unsigned FULL = 0xffffffffu;
@@ -396,6 +397,8 @@ __global__ void __launch_bounds__(kTraceBlock, 4) k_trace(TraceArgs A) {
     bool active = false;
     bool exhausted = false;  // warp-uniform: the cursor has passed the end of the work list
     int item = 0;
+    // Every lane of the warp runs every phase below (lanes without a ray or without work for
+    // a phase are predicated off), so the ballots see the whole warp.
     while (true) {
         unsigned need = __ballot_sync(FULL, !active);
         if (need && !exhausted) {
@@ -443,9 +446,34 @@ __global__ void __launch_bounds__(kTraceBlock, 4) k_trace(TraceArgs A) {
             }
         }
         if (!__any_sync(FULL, active)) break;
-        while (active) {
-            T.step(L);
-            if (L.done) {
+        while (true) {
+            // node phase
+            if (active && (L.g.y & 0xffu)) T.visit(L);
+            // triangle phase, postponed while too few lanes have triangles and others nodes
+            while (true) {
+                const bool want = active && (L.t.y & kTagMask) == kTagTri;
+                const unsigned wm = __ballot_sync(FULL, want);
+                if (!wm) break;
+                const bool nodes = active && (L.g.y & 0xffu);
+                if (__popc(wm) < kPostpone && __any_sync(FULL, nodes)) {
+                    // lanes with nodes left push their triangles; the others keep them
+                    if (want && nodes) {
+                        T.push(L, L.t);
+                        L.t = make_uint2(0u, 0u);
+                    }
+                    break;
+                }
+                if (want) T.test_one(L);
+                if (MODE == 2 && want && L.done) {
+                    L.t = make_uint2(0u, 0u);
+                    L.g = make_uint2(0u, 0u);
+                }
+            }
+            // instance phase
+            if (active && !L.done && (L.t.y & kTagMask) == kTagInst) T.enter(L);
+            // pop phase
+            if (active && !L.done && !(L.g.y & 0xffu) && !(L.t.y & kRecMask)) T.next(L);
+            if (active && L.done) {
                 active = false;
                 if (ext) {
                     uint32_t* h = A.ext_hits + size_t(item) * 5;
@@ -467,7 +495,7 @@ __global__ void __launch_bounds__(kTraceBlock, 4) k_trace(TraceArgs A) {
                     if (hit && A.nee) {
                         // shadow ray of the raygen program (src/optixshaders/optix_triangle.cu:82-132)
                         f3 n = hit_world_normal(A.S, L.best.inst, L.best.prim, L.best.u, L.best.v);
-                        f3 wo = L.world.o, wd = L.world.d;
+                        f3 wo = L.wo, wd = L.wd;
                         f3 hp = mk(__fadd_rn(wo.x, __fmul_rn(L.best.t, wd.x)), __fadd_rn(wo.y, __fmul_rn(L.best.t, wd.y)),
                                    __fadd_rn(wo.z, __fmul_rn(L.best.t, wd.z)));
                         f3 so = mk(__fadd_rn(hp.x, __fmul_rn(n.x, 1e-4f)), __fadd_rn(hp.y, __fmul_rn(n.y, 1e-4f)),
@@ -503,9 +531,10 @@ __global__ void __launch_bounds__(kTraceBlock, 4) k_trace(TraceArgs A) {
                 } else {
                     A.W.sh_hit[item] = make_float4(L.best.inst >= 0 ? 1.0f : -1.0f, 0.0f, 0.0f, __int_as_float(-1));
                 }
-                break;
             }
-            if (__popc(__activemask()) < kRefill && !exhausted) break;
+            const unsigned am = __ballot_sync(FULL, active);
+            if (!am) break;
+            if (__popc(am) < kRefill && !exhausted) break;
         }
     }
 }
