@@ -35,7 +35,7 @@ namespace {
 
 constexpr int kShStack = 16;
 constexpr int kLocStack = 48;
-constexpr int kRefill = 20;
+constexpr int kRefill = 24;
 constexpr uint32_t kTagMask = 3u << 30;
 constexpr uint32_t kTagNode = 0u;
 constexpr uint32_t kTagTri = 1u << 30;
@@ -43,8 +43,9 @@ constexpr uint32_t kTagInst = 2u << 30;
 constexpr uint32_t kTagMarker = 3u << 30;
 constexpr uint32_t kRecMask = 0xffffffu;
 // fewer lanes than this with triangles to test: push the triangle groups and keep
-// traversing nodes (the postponement of Ylitie et al. 2017)
-constexpr int kPostpone = 8;
+// traversing nodes (the postponement of Ylitie et al. 2017); 4 and a refill threshold of 24
+// lanes were the fastest of the values tried on the 1M-triangle 1080p workload
+constexpr int kPostpone = 4;
 constexpr float kLo = 1.0f - 1.0f / 524288.0f;
 constexpr float kHi = 1.0f + 1.0f / 524288.0f;
 
@@ -375,7 +376,9 @@ LUX_DI f3 hit_world_normal(const DevScene& S, int inst, int prim, float bu, floa
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kTraceBlock, 6) k_trace(TraceArgs A) {
+// The arguments stay in parameter space (__grid_constant__): the tracer reads the scene
+// through a reference to them, which would otherwise copy the struct to local memory.
+__global__ void __launch_bounds__(kTraceBlock, 6) k_trace(const __grid_constant__ TraceArgs A) {
     __shared__ uint2 stack[kShStack][kTraceBlock];
     Tracer<MODE> T{A.S, stack, {}, int(threadIdx.x), &A.W.ctr->error};
     const unsigned FULL = 0xffffffffu;
