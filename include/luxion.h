@@ -223,6 +223,12 @@ typedef struct lux_stats {
 int lux_enable_timing(lux_ctx* ctx, int on);
 int lux_get_stats(lux_ctx* ctx, lux_stats* out);
 
+/* Queue lengths of the last wave rendered: paths[b] = paths entering bounce b (paths[0] = the
+ * wave's camera paths; paths[b+1] = survivors of bounce b, the reference's num_paths after the
+ * compaction of src/pathtrace.cu:316-322), shadow[b] = shadow rays traced at bounce b. Entries
+ * up to max_bounces are written (the rest of each array is left alone). */
+int lux_wave_counts(lux_ctx* ctx, int* paths, int* shadow, int max_bounces);
+
 /* ---- kernel-level entry points used by the parity suite --------------------------------- */
 
 /* Closest-hit / any-hit trace of caller rays through the device BVH.

@@ -44,6 +44,7 @@ SIGNATURES = {
     "lux_last_error": (C.c_char_p, []),
     "lux_enable_timing": (C.c_int, [_P, C.c_int]),
     "lux_get_stats": (C.c_int, [_P, C.POINTER(Stats)]),
+    "lux_wave_counts": (C.c_int, [_P, c_int_p, c_int_p, C.c_int]),
     "lux_trace_rays": (C.c_int, [_P, c_float_p, C.c_int, C.c_int, C.c_int, c_u32_p]),
     "lux_trace_rays_static": (C.c_int, [_P, c_float_p, C.c_int, C.c_int, C.c_int, c_u32_p]),
     "lux_morton_keys": (C.c_int, [_P, c_float_p, C.c_int, c_u32_p]),
@@ -195,6 +196,13 @@ class Renderer:
         s = Stats()
         _check(lib().lux_get_stats(self._h, C.byref(s)))
         return {n: getattr(s, n) for n, _ in Stats._fields_}
+
+    def wave_counts(self, max_bounces: int = 64):
+        """(paths entering each bounce, shadow rays per bounce) of the last wave rendered."""
+        p = np.zeros(max_bounces, np.int32)
+        sh = np.zeros(max_bounces, np.int32)
+        _check(lib().lux_wave_counts(self._h, ptr(p, C.c_int), ptr(sh, C.c_int), max_bounces))
+        return p, sh
 
     # kernel-level entry points (parity suite)
     def trace_rays(self, rays: np.ndarray, mode: int = 0, it: int = 1) -> np.ndarray:

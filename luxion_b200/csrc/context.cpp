@@ -1037,6 +1037,20 @@ int lux_get_stats(lux_ctx* C, lux_stats* out) {
     return LUX_OK;
 }
 
+int lux_wave_counts(lux_ctx* C, int* paths, int* shadow, int max_bounces) {
+    if (!C || !paths || !shadow || max_bounces < 0) return fail(LUX_ERR_INVALID, "bad arguments");
+    LUX_CUDA(cudaSetDevice(C->device));
+    WaveCounters hc;
+    LUX_CUDA(cudaMemcpyAsync(&hc, C->W.ctr, sizeof(hc), cudaMemcpyDeviceToHost, C->stream));
+    LUX_CUDA(cudaStreamSynchronize(C->stream));
+    const int n = std::min(max_bounces, kMaxDepth);
+    for (int b = 0; b < n; ++b) {
+        paths[b] = hc.count[b];
+        shadow[b] = hc.shadow[b];
+    }
+    return LUX_OK;
+}
+
 // ---- kernel-level entry points -------------------------------------------------------
 int lux_trace_rays(lux_ctx* C, const float* rays, int n, int mode, int iter, uint32_t* hits) {
     if (!C || (!rays && n > 0) || (!hits && n > 0) || n < 0 || mode < 0 || mode > 2)
