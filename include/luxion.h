@@ -293,6 +293,88 @@ int lux_rng_stream(int iter, int index, int depth, int n, float* out);
  * pairs; out n*4 floats. */
 int lux_sample_texture(lux_ctx* ctx, int tex, const float* uv, int n, float* out);
 
+/* ---- job engine: many render jobs in one shared wavefront (no counterpart in the reference)
+ *
+ * The batching and serving forms. An engine keeps several scenes resident on one device
+ * (their acceleration structures, materials, textures and light tables concatenated) and
+ * renders any number of jobs -- each a scene, a camera with its own resolution, a sample count
+ * and a trace depth -- in waves whose paths come from many jobs at once. Every wave is one
+ * graph replay: camera rays for the wave's job segments, depth x (trace, shade, shadow trace),
+ * and a per-job accumulation in sample order. A job's image is therefore the same bit for bit
+ * whether it renders alone or among others, and the same as lux_render of that scene and
+ * camera in a single-job context. Lighting options (-dmis, -emis, envmap intensity, precision,
+ * texture storage) are the engine's; ray sorting is not used.
+ * Jobs are admitted in submission order while the engine's device memory (scenes + wave
+ * buffers + admitted jobs' images) stays within hbm_budget_bytes; the others wait queued.
+ * An engine is driven by one host thread. */
+typedef struct lux_engine lux_engine;
+
+typedef struct lux_job_desc {
+    int32_t scene;            /* index of a resident scene                                     */
+    int32_t spp;              /* samples per pixel                                             */
+    int32_t trace_depth;      /* 0: the scene's trace_depth                                    */
+    int32_t first_iter;       /* iteration of the first sample (1-based, the reference's iter); 0 = 1 */
+    lux_camera_desc camera;   /* resolution and pose                                           */
+} lux_job_desc;
+
+enum { LUX_SCHED_FIFO = 0, LUX_SCHED_SHORTEST_FIRST = 1 };
+
+typedef struct lux_engine_config {
+    int64_t hbm_budget_bytes; /* admission limit on the engine's device memory; 0 = unlimited   */
+    int32_t max_paths;        /* paths per wave; 0 = autotune over a few sizes on the first waves */
+    int32_t max_jobs;         /* job table capacity (live jobs); 0 = 4096                       */
+    int32_t schedule;         /* LUX_SCHED_*: order in which admitted jobs fill a wave            */
+    int32_t trace_blocks;     /* persistent trace grid in blocks; 0 = full occupancy (autotuned with max_paths) */
+} lux_engine_config;
+
+enum { LUX_JOB_QUEUED = 0, LUX_JOB_ACTIVE = 1, LUX_JOB_DONE = 2, LUX_JOB_RELEASED = 3 };
+
+typedef struct lux_job_status {
+    int32_t state;            /* LUX_JOB_*                                                     */
+    int32_t spp_done;         /* samples accumulated so far (a progressive result)             */
+    int32_t spp;
+    int32_t waves;            /* waves the job took part in                                     */
+    double t_submit_ms, t_admit_ms, t_done_ms;   /* engine clock (ms since creation)            */
+} lux_job_status;
+
+typedef struct lux_engine_stats {
+    int64_t waves;
+    double samples;           /* pixel samples rendered                                         */
+    double rays;              /* radiance + shadow rays traced                                  */
+    double ms_device;         /* summed wave times (CUDA events)                                */
+    int64_t device_bytes;     /* scenes + wave buffers + live job images                        */
+    int64_t scene_bytes;
+    int32_t max_paths;        /* wave size in use (autotuned when configured 0)                 */
+    int32_t trace_blocks;     /* persistent trace grid in use                                   */
+    int32_t jobs_queued, jobs_active, jobs_done;
+} lux_engine_stats;
+
+int lux_engine_create(const lux_scene_desc* const* scenes, int num_scenes, const lux_options* opt,
+                      const lux_engine_config* cfg, lux_engine** out);
+/* Queue a job; *job_id identifies it from then on. */
+int lux_engine_submit(lux_engine* e, const lux_job_desc* job, int* job_id);
+/* Admit what fits, render one wave, and return how many jobs completed in it (*done_jobs may
+ * be NULL). *idle is set to 1 when there was nothing to render. */
+int lux_engine_step(lux_engine* e, int* done_jobs, int* idle);
+/* Step until every submitted job is done. */
+int lux_engine_run(lux_engine* e);
+int lux_engine_job_status(lux_engine* e, int job_id, lux_job_status* out);
+/* The job's FP32 accumulation sum (width*height*3), at any point of its progress. */
+int lux_engine_copy_image(lux_engine* e, int job_id, float* rgb_host);
+/* Free a finished (or queued) job's device memory. */
+int lux_engine_release(lux_engine* e, int job_id);
+int lux_engine_get_stats(lux_engine* e, lux_engine_stats* out);
+/* The engine clock (ms since creation), the time base of lux_job_status. */
+double lux_engine_clock_ms(lux_engine* e);
+int lux_engine_free(lux_engine* e);
+
+/* Pure wave planner (host only, used by the engine; exposed for tests): given each live job's
+ * pixels per sample and samples left, in the order they may fill the wave, choose how many
+ * samples each contributes to a wave of `capacity` paths with at most `max_segments` segments.
+ * A job contributes only whole samples and only if at least one fits. Returns the number of
+ * segments; take[i] receives job i's samples. */
+int lux_plan_wave(const int* npix, const int* remaining, int njobs, int capacity, int max_segments, int* take);
+
 /* ---- procedural scenes (host only; no device needed) ------------------------------------ */
 typedef struct lux_host_scene lux_host_scene;
 

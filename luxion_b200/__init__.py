@@ -22,8 +22,8 @@ from typing import Optional
 import numpy as np
 
 from . import _ffi
-from ._ffi import (CameraDesc, Options, RandomSceneParams, SceneDesc, Stats, c_float_p, c_int_p,
-                   c_u32_p, default_options)
+from ._ffi import (CameraDesc, EngineConfig, EngineStats, JobDesc, JobStatus, Options, RandomSceneParams,
+                   SceneDesc, Stats, c_float_p, c_int_p, c_u32_p, default_options)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_lib", "libluxion.so")
@@ -53,6 +53,18 @@ SIGNATURES = {
     "lux_get_cdfs": (C.c_int, [_P, c_float_p, c_float_p, c_float_p, c_float_p, c_float_p]),
     "lux_rng_stream": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, c_float_p]),
     "lux_sample_texture": (C.c_int, [_P, C.c_int, c_float_p, C.c_int, c_float_p]),
+    "lux_engine_create": (C.c_int, [C.POINTER(C.POINTER(SceneDesc)), C.c_int, C.POINTER(Options),
+                                    C.POINTER(EngineConfig), C.POINTER(_P)]),
+    "lux_engine_submit": (C.c_int, [_P, C.POINTER(JobDesc), c_int_p]),
+    "lux_engine_step": (C.c_int, [_P, c_int_p, c_int_p]),
+    "lux_engine_run": (C.c_int, [_P]),
+    "lux_engine_job_status": (C.c_int, [_P, C.c_int, C.POINTER(JobStatus)]),
+    "lux_engine_copy_image": (C.c_int, [_P, C.c_int, c_float_p]),
+    "lux_engine_release": (C.c_int, [_P, C.c_int]),
+    "lux_engine_get_stats": (C.c_int, [_P, C.POINTER(EngineStats)]),
+    "lux_engine_clock_ms": (C.c_double, [_P]),
+    "lux_engine_free": (C.c_int, [_P]),
+    "lux_plan_wave": (C.c_int, [c_int_p, c_int_p, C.c_int, C.c_int, C.c_int, c_int_p]),
     "lux_scene_cornell36": (_P, [C.c_int, C.c_int]),
     "lux_default_random_scene_params": (None, [C.POINTER(RandomSceneParams)]),
     "lux_scene_random": (_P, [C.POINTER(RandomSceneParams)]),
@@ -270,6 +282,91 @@ class Renderer:
             self.close()
         except Exception:
             pass
+
+
+class Engine:
+    """The job engine (lux_engine_*): resident scenes, many jobs in one shared wavefront.
+
+    Each scene is a HostScene or SceneBuilder (anything with desc_ptr). A job is a scene index,
+    a camera (defaulting to the scene's own), samples per pixel and a trace depth; its image
+    equals the single-job render of the same scene, camera and samples bit for bit."""
+
+    def __init__(self, scenes, options: Optional[Options] = None, hbm_budget_bytes: int = 0, max_paths: int = 0,
+                 max_jobs: int = 0, schedule: int = _ffi.SCHED_FIFO, trace_blocks: int = 0):
+        self._scenes = list(scenes)
+        ptrs = (C.POINTER(SceneDesc) * len(self._scenes))(*[sc.desc_ptr for sc in self._scenes])
+        self.options = options if options is not None else default_options()
+        cfg = EngineConfig()
+        cfg.hbm_budget_bytes, cfg.max_paths, cfg.max_jobs = hbm_budget_bytes, max_paths, max_jobs
+        cfg.schedule, cfg.trace_blocks = schedule, trace_blocks
+        h = _P()
+        _check(lib().lux_engine_create(ptrs, len(self._scenes), C.byref(self.options), C.byref(cfg), C.byref(h)))
+        self._h = h
+        self._sizes = {}
+
+    def submit(self, scene: int, spp: int, trace_depth: int = 0, first_iter: int = 1,
+               camera: Optional[CameraDesc] = None) -> int:
+        j = JobDesc()
+        j.scene, j.spp, j.trace_depth, j.first_iter = scene, spp, trace_depth, first_iter
+        j.camera = camera if camera is not None else self._scenes[scene].desc.camera
+        jid = C.c_int()
+        _check(lib().lux_engine_submit(self._h, C.byref(j), C.byref(jid)))
+        self._sizes[jid.value] = (j.camera.height, j.camera.width)
+        return jid.value
+
+    def step(self):
+        """Render one wave; returns (jobs completed in it, idle)."""
+        done, idle = C.c_int(), C.c_int()
+        _check(lib().lux_engine_step(self._h, C.byref(done), C.byref(idle)))
+        return done.value, bool(idle.value)
+
+    def run(self):
+        _check(lib().lux_engine_run(self._h))
+
+    def status(self, job: int) -> dict:
+        st = JobStatus()
+        _check(lib().lux_engine_job_status(self._h, job, C.byref(st)))
+        return {n: getattr(st, n) for n, _ in JobStatus._fields_}
+
+    def image(self, job: int) -> np.ndarray:
+        h, w = self._sizes[job]
+        out = np.empty((h, w, 3), np.float32)
+        _check(lib().lux_engine_copy_image(self._h, job, ptr(out)))
+        return out
+
+    def release(self, job: int):
+        _check(lib().lux_engine_release(self._h, job))
+
+    def stats(self) -> dict:
+        st = EngineStats()
+        _check(lib().lux_engine_get_stats(self._h, C.byref(st)))
+        return {n: getattr(st, n) for n, _ in EngineStats._fields_}
+
+    def clock_ms(self) -> float:
+        return float(lib().lux_engine_clock_ms(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().lux_engine_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def plan_wave(npix, remaining, capacity: int, max_segments: int = 256) -> np.ndarray:
+    """The engine's wave planner (lux_plan_wave): samples each job contributes to one wave."""
+    npix = np.ascontiguousarray(npix, np.int32)
+    remaining = np.ascontiguousarray(remaining, np.int32)
+    take = np.zeros(len(npix), np.int32)
+    rc = lib().lux_plan_wave(ptr(npix, C.c_int), ptr(remaining, C.c_int), len(npix), capacity, max_segments,
+                             ptr(take, C.c_int))
+    if rc < 0:
+        _check(rc)
+    return take
 
 
 def rng_stream(it: int, index: int, depth: int, n: int) -> np.ndarray:

@@ -107,6 +107,32 @@ class RandomSceneParams(C.Structure):
                 ("tex_half", C.c_int32)]
 
 
+class JobDesc(C.Structure):
+    _fields_ = [("scene", C.c_int32), ("spp", C.c_int32), ("trace_depth", C.c_int32),
+                ("first_iter", C.c_int32), ("camera", CameraDesc)]
+
+
+SCHED_FIFO, SCHED_SHORTEST_FIRST = 0, 1
+JOB_QUEUED, JOB_ACTIVE, JOB_DONE, JOB_RELEASED = 0, 1, 2, 3
+
+
+class EngineConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_int64), ("max_paths", C.c_int32), ("max_jobs", C.c_int32),
+                ("schedule", C.c_int32), ("trace_blocks", C.c_int32)]
+
+
+class JobStatus(C.Structure):
+    _fields_ = [("state", C.c_int32), ("spp_done", C.c_int32), ("spp", C.c_int32), ("waves", C.c_int32),
+                ("t_submit_ms", C.c_double), ("t_admit_ms", C.c_double), ("t_done_ms", C.c_double)]
+
+
+class EngineStats(C.Structure):
+    _fields_ = [("waves", C.c_int64), ("samples", C.c_double), ("rays", C.c_double), ("ms_device", C.c_double),
+                ("device_bytes", C.c_int64), ("scene_bytes", C.c_int64), ("max_paths", C.c_int32),
+                ("trace_blocks", C.c_int32), ("jobs_queued", C.c_int32), ("jobs_active", C.c_int32),
+                ("jobs_done", C.c_int32)]
+
+
 def default_options(**kw) -> Options:
     """PathTracerOptions defaults (include/pathtrace/pathtracer_options.h:3-11)."""
     o = Options()

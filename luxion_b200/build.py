@@ -9,7 +9,7 @@ Translation units:
               rounded on its own, in the reference's order
   sort.cu     Morton keys and the radix sort of a bounce queue
   trace_static.cu  the fixed device scratch of lux_trace_rays_static
-  context.cpp, bvh_build.cpp, scene_gen.cpp   host C++ (no FMA contraction)
+  context.cpp, engine.cpp, bvh_build.cpp, scene_gen.cpp   host C++ (no FMA contraction)
 The CUDA runtime is linked statically so the library does not depend on which libcudart a
 host process (for example PyTorch) has already loaded.
 """
@@ -37,7 +37,7 @@ CU_UNITS = {
     "sort.cu": ["--fmad=true"],
     "trace_static.cu": ["--fmad=true"],
 }
-CPP_UNITS = ["context.cpp", "bvh_build.cpp", "scene_gen.cpp"]
+CPP_UNITS = ["context.cpp", "engine.cpp", "bvh_build.cpp", "scene_gen.cpp"]
 
 
 def _sources():

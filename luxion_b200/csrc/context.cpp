@@ -18,6 +18,7 @@
 #include "bvh8.h"
 #include "device_scene.h"
 #include "launch.h"
+#include "host_common.h"
 
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -35,7 +36,7 @@
 
 using namespace lux;
 
-namespace {
+namespace lux {
 
 thread_local std::string g_err;
 
@@ -44,36 +45,9 @@ int fail(int code, const std::string& msg) {
     return code;
 }
 
-#define LUX_CUDA(call)                                                                      \
-    do {                                                                                    \
-        cudaError_t e_ = (call);                                                            \
-        if (e_ != cudaSuccess) {                                                            \
-            return fail(e_ == cudaErrorMemoryAllocation ? LUX_ERR_OOM : LUX_ERR_CUDA,       \
-                        std::string(#call) + ": " + cudaGetErrorString(e_));                \
-        }                                                                                   \
-    } while (0)
+}  // namespace lux
 
-template <class T>
-int dalloc(T** p, size_t n) {
-    *p = nullptr;
-    if (n == 0) return LUX_OK;
-    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(T));
-    if (e != cudaSuccess) return fail(LUX_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-    return LUX_OK;
-}
-template <class T>
-int upload(T** p, const T* src, size_t n) {
-    int rc = dalloc(p, n);
-    if (rc) return rc;
-    if (n) LUX_CUDA(cudaMemcpy(*p, src, n * sizeof(T), cudaMemcpyHostToDevice));
-    return LUX_OK;
-}
-
-struct DevTex {
-    cudaArray_t arr = nullptr;
-    cudaTextureObject_t obj = 0;
-    size_t bytes = 0;
-};
+namespace {
 
 bool invert4(const float* m, double* out) {
     double t[4][8];
@@ -341,7 +315,10 @@ bool light_tables(const lux_scene_desc& d, const std::vector<float>& env, std::v
     return true;
 }
 
-int build_scene(lux_ctx* C, const lux_scene_desc& d) {
+}  // namespace
+
+int lux::build_host_scene(const lux_scene_desc& d, const lux_options& opt, std::vector<DevTex>& texs,
+                          DevTex& env, HostScene& H) {
     // ---- per-mesh BLAS (threaded across meshes) ----
     const int NM = d.num_meshes;
     std::vector<BVH8Build> blas(NM);
@@ -380,14 +357,15 @@ int build_scene(lux_ctx* C, const lux_scene_desc& d) {
         for (auto& t : th) t.join();
     }
     // ---- concatenate meshes ----
-    std::vector<BVH8Node> nodes;
-    std::vector<float4> prims;
-    std::vector<float> pos, nrm, uv;
-    std::vector<uint32_t> idx;
+    std::vector<BVH8Node>& nodes = H.nodes;
+    std::vector<float4>& prims = H.prims;
+    std::vector<float>&pos = H.pos, &nrm = H.nrm, &uv = H.uv;
+    std::vector<uint32_t>& idx = H.idx;
     std::vector<uint32_t> mesh_root(NM), mesh_prim(NM), mesh_vert(NM), mesh_idx(NM);
     std::vector<int> mesh_flags(NM);
     std::vector<float> mesh_box(size_t(NM) * 6);
-    bool any_n = false, any_uv = false;
+    bool& any_n = H.any_n;
+    bool& any_uv = H.any_uv;
     for (int m = 0; m < NM; ++m) {
         any_n |= d.meshes[m].normals != nullptr;
         any_uv |= d.meshes[m].uvs != nullptr;
@@ -441,9 +419,10 @@ int build_scene(lux_ctx* C, const lux_scene_desc& d) {
     }
     // ---- instances + TLAS ----
     const int NI = d.num_instances;
-    std::vector<DevInstance> insts(NI);
+    std::vector<DevInstance>& insts = H.insts;
+    insts.assign(NI, DevInstance{});
     std::vector<float> iboxes(size_t(NI) * 6);
-    C->instanced_tris = 0;
+    H.instanced_tris = 0;
     for (int i = 0; i < NI; ++i) {
         const lux_instance_desc& in = d.instances[i];
         DevInstance& I = insts[i];
@@ -473,7 +452,8 @@ int build_scene(lux_ctx* C, const lux_scene_desc& d) {
         const lux_material_desc& mat = d.materials[in.material];
         I.flags = mesh_flags[in.mesh] | (mat.alpha_mode != LUX_ALPHA_OPAQUE ? kInstAnyHit : 0);
         I.num_tris = d.meshes[in.mesh].num_tris;
-        C->instanced_tris += I.num_tris;
+        I.key = i;
+        H.instanced_tris += I.num_tris;
         // world box: 8 transformed corners of the mesh box, in double, padded
         const float* mb = &mesh_box[size_t(in.mesh) * 6];
         float* b = &iboxes[size_t(i) * 6];
@@ -501,20 +481,23 @@ int build_scene(lux_ctx* C, const lux_scene_desc& d) {
     BVH8Build tl;
     build_bvh8(iboxes.data(), NI, tl);
     uint32_t tlas_root = uint32_t(nodes.size());
+    H.tlas_root = tlas_root;
     for (BVH8Node n : tl.nodes) {
         n.child_base += tlas_root;
         nodes.push_back(n);
     }
-    std::vector<uint32_t> tlas_prims(tl.prim_order.begin(), tl.prim_order.end());
+    H.tlas_prims.assign(tl.prim_order.begin(), tl.prim_order.end());
     if (tl.depth + max_blas_depth + 4 > 16 + 48)
         return fail(LUX_ERR_UNSUPPORTED, "acceleration structure deeper than the traversal stack");
     // ---- materials + textures ----
-    C->texs.resize(d.num_textures);
+    const size_t tex0 = texs.size();
+    texs.resize(tex0 + d.num_textures);
     for (int t = 0; t < d.num_textures; ++t) {
-        int rc = make_texture(d.textures[t], C->texs[t], C->opt.texture_storage);
+        int rc = make_texture(d.textures[t], texs[tex0 + t], opt.texture_storage);
         if (rc) return rc;
     }
-    std::vector<DevMaterial> mats(d.num_materials);
+    std::vector<DevMaterial>& mats = H.mats;
+    mats.assign(d.num_materials, DevMaterial{});
     for (int k = 0; k < d.num_materials; ++k) {
         const lux_material_desc& s = d.materials[k];
         DevMaterial& m = mats[k];
@@ -533,7 +516,7 @@ int build_scene(lux_ctx* C, const lux_scene_desc& d) {
         auto tex_of = [&](int t, int flag, unsigned long long& obj) -> int {
             if (t < 0) return LUX_OK;
             if (t >= d.num_textures) return fail(LUX_ERR_INVALID, "material texture index out of range");
-            obj = C->texs[t].obj;
+            obj = texs[tex0 + t].obj;
             m.flags |= flag;
             return LUX_OK;
         };
@@ -556,98 +539,60 @@ int build_scene(lux_ctx* C, const lux_scene_desc& d) {
     }
     // ---- light tables ----
     std::vector<float> envt;
-    if (d.env_data) env_texels(d, C->opt.texture_storage, envt);
-    std::vector<int> emissive;
+    if (d.env_data) env_texels(d, opt.texture_storage, envt);
     std::vector<std::vector<float>> tri_prefix;
     bool env_ok;
-    if (C->opt.precision == LUX_PRECISION_COMPENSATED)
-        env_ok = light_tables<double>(d, envt, emissive, C->h_emissive_prefix, tri_prefix, C->h_total_area,
-                                      C->h_marginal, C->h_conditional);
+    if (opt.precision == LUX_PRECISION_COMPENSATED)
+        env_ok = light_tables<double>(d, envt, H.emissive, H.emissive_prefix, tri_prefix, H.total_area, H.marginal,
+                                      H.conditional);
     else
-        env_ok = light_tables<float>(d, envt, emissive, C->h_emissive_prefix, tri_prefix, C->h_total_area,
-                                     C->h_marginal, C->h_conditional);
+        env_ok = light_tables<float>(d, envt, H.emissive, H.emissive_prefix, tri_prefix, H.total_area, H.marginal,
+                                     H.conditional);
     if (!env_ok) return fail(LUX_ERR_INVALID, "environment map has no emission");
-    std::vector<int> tri_off;
-    C->h_tri_prefix.clear();
-    for (int e : emissive) {
-        tri_off.push_back(int(C->h_tri_prefix.size()));
-        C->h_tri_prefix.insert(C->h_tri_prefix.end(), tri_prefix[e].begin(), tri_prefix[e].end());
+    H.tri_off.clear();
+    H.tri_prefix.clear();
+    for (int e : H.emissive) {
+        H.tri_off.push_back(int(H.tri_prefix.size()));
+        H.tri_prefix.insert(H.tri_prefix.end(), tri_prefix[e].begin(), tri_prefix[e].end());
     }
-    if (C->opt.direct_light_sampling && (emissive.empty() || C->h_total_area < 0.00001f))
+    if (opt.direct_light_sampling && (H.emissive.empty() || H.total_area < 0.00001f))
         return fail(LUX_ERR_INVALID, "-dmis requires the scene to contain emissive geometry");
-    if (C->opt.env_importance_sampling && !d.env_data)
+    if (opt.env_importance_sampling && !d.env_data)
         return fail(LUX_ERR_INVALID, "-emis requires an environment map");
     if (d.env_data) {
         lux_texture_desc et{d.env_width, d.env_height, d.env_format, 0, d.env_data};
-        int rc = make_texture(et, C->env, C->opt.texture_storage == LUX_TEXSTORE_HALF ? LUX_TEXSTORE_HALF : LUX_TEXSTORE_FLOAT);
+        int rc = make_texture(et, env, opt.texture_storage == LUX_TEXSTORE_HALF ? LUX_TEXSTORE_HALF : LUX_TEXSTORE_FLOAT);
         if (rc) return rc;
-    }
-    // ---- upload ----
-    DevScene& S = C->S;
-    std::memset(&S, 0, sizeof(S));
-    uint4* dn = nullptr;
-    int rc = C->up(&dn, reinterpret_cast<const uint4*>(nodes.data()), nodes.size() * 5);
-    if (rc) return rc;
-    S.nodes = dn;
-    float4* dp = nullptr;
-    if ((rc = C->up(&dp, prims.data(), prims.size()))) return rc;
-    S.prims = dp;
-    DevInstance* di = nullptr;
-    if ((rc = C->up(&di, insts.data(), insts.size()))) return rc;
-    S.insts = di;
-    uint32_t* dt = nullptr;
-    if ((rc = C->up(&dt, tlas_prims.data(), tlas_prims.size()))) return rc;
-    S.tlas_prims = dt;
-    S.tlas_root = tlas_root;
-    S.num_insts = NI;
-    float* f = nullptr;
-    if ((rc = C->up(&f, pos.data(), pos.size()))) return rc;
-    S.pos = f;
-    if (any_n) {
-        if ((rc = C->up(&f, nrm.data(), nrm.size()))) return rc;
-        S.nrm = f;
-    }
-    if (any_uv) {
-        if ((rc = C->up(&f, uv.data(), uv.size()))) return rc;
-        S.uv = f;
-    }
-    uint32_t* du = nullptr;
-    if ((rc = C->up(&du, idx.data(), idx.size()))) return rc;
-    S.idx = du;
-    DevMaterial* dm = nullptr;
-    if ((rc = C->up(&dm, mats.data(), mats.size()))) return rc;
-    S.mats = dm;
-    int* ei = nullptr;
-    if ((rc = C->up(&ei, emissive.data(), emissive.size()))) return rc;
-    S.emissive_inst = ei;
-    if ((rc = C->up(&f, C->h_emissive_prefix.data(), C->h_emissive_prefix.size()))) return rc;
-    S.emissive_prefix = f;
-    if ((rc = C->up(&f, C->h_tri_prefix.data(), C->h_tri_prefix.size()))) return rc;
-    S.tri_prefix = f;
-    if ((rc = C->up(&ei, tri_off.data(), tri_off.size()))) return rc;
-    S.tri_prefix_off = ei;
-    S.num_emissive = int(emissive.size());
-    S.total_area = C->h_total_area;
-    if (d.env_data) {
-        if ((rc = C->up(&f, C->h_marginal.data(), C->h_marginal.size()))) return rc;
-        S.marginal = f;
-        if ((rc = C->up(&f, C->h_conditional.data(), C->h_conditional.size()))) return rc;
-        S.conditional = f;
-        S.env_w = d.env_width;
-        S.env_h = d.env_height;
-        S.env_tex = C->env.obj;
-        S.has_env = 1;
+        H.env_w = d.env_width;
+        H.env_h = d.env_height;
+        H.env_tex = env.obj;
+        H.has_env = true;
     }
     // Morton box: the first instance's mesh bounds padded by 1e-5 (EPSILON of
     // include/utilities.h:16), in that instance's object space
     if (NI > 0) {
         const float* mb = &mesh_box[size_t(d.instances[0].mesh) * 6];
         for (int a = 0; a < 3; ++a) {
-            S.morton_bmin[a] = mb[a] - 0.00001f;
-            S.morton_bmax[a] = mb[3 + a] + 0.00001f;
+            H.morton_bmin[a] = mb[a] - 0.00001f;
+            H.morton_bmax[a] = mb[3 + a] + 0.00001f;
         }
     }
     return LUX_OK;
+}
+
+namespace {
+
+int build_scene(lux_ctx* C, const lux_scene_desc& d) {
+    HostScene H;
+    int rc = build_host_scene(d, C->opt, C->texs, C->env, H);
+    if (rc) return rc;
+    C->instanced_tris = H.instanced_tris;
+    C->h_emissive_prefix = H.emissive_prefix;
+    C->h_tri_prefix = H.tri_prefix;
+    C->h_marginal = H.marginal;
+    C->h_conditional = H.conditional;
+    C->h_total_area = H.total_area;
+    return upload_scene(C, H, C->S);
 }
 
 int alloc_wave(lux_ctx* C, int max_paths) {
@@ -823,24 +768,7 @@ struct Tmp {
 
 }  // namespace
 
-extern "C" {
-
-void lux_default_options(lux_options* o) {
-    if (!o) return;
-    std::memset(o, 0, sizeof(*o));
-    o->color_mode = LUX_TONEMAP_ACES;
-    o->envmap_intensity = 1.0f;
-    o->use_graph = 1;
-    o->texture_storage = LUX_TEXSTORE_FLOAT;
-}
-
-const char* lux_last_error(void) { return g_err.c_str(); }
-
-int lux_init(const lux_scene_desc* scene, const lux_options* opt, lux_ctx** out) {
-    if (!out) return fail(LUX_ERR_INVALID, "out is NULL");
-    *out = nullptr;
-    if (!scene) return fail(LUX_ERR_INVALID, "scene is NULL");
-    const lux_scene_desc& d = *scene;
+int lux::validate_scene_desc(const lux_scene_desc& d) {
     if (d.num_instances <= 0 || d.num_meshes <= 0 || !d.meshes || !d.instances)
         return fail(LUX_ERR_INVALID, "scene has no geometry");
     if (d.num_materials <= 0 || !d.materials) return fail(LUX_ERR_INVALID, "scene has no materials");
@@ -862,6 +790,28 @@ int lux_init(const lux_scene_desc* scene, const lux_options* opt, lux_ctx** out)
     if (d.env_data && (d.env_width <= 0 || d.env_height <= 0 ||
                        (d.env_format != LUX_TEX_RGBA32F && d.env_format != LUX_TEX_RGBA16F)))
         return fail(LUX_ERR_INVALID, "environment map must be RGBA32F or RGBA16F with a positive size");
+    return LUX_OK;
+}
+
+extern "C" {
+
+void lux_default_options(lux_options* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->color_mode = LUX_TONEMAP_ACES;
+    o->envmap_intensity = 1.0f;
+    o->use_graph = 1;
+    o->texture_storage = LUX_TEXSTORE_FLOAT;
+}
+
+const char* lux_last_error(void) { return lux::g_err.c_str(); }
+
+int lux_init(const lux_scene_desc* scene, const lux_options* opt, lux_ctx** out) {
+    if (!out) return fail(LUX_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!scene) return fail(LUX_ERR_INVALID, "scene is NULL");
+    const lux_scene_desc& d = *scene;
+    if (int rc = validate_scene_desc(d)) return rc;
     lux_options o;
     if (opt) o = *opt;
     else lux_default_options(&o);

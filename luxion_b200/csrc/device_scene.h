@@ -35,6 +35,7 @@ struct DevInstance {
     uint32_t idx_base;    // first index triplet of the mesh
     int flags;            // InstFlags
     int num_tris;
+    int key;              // index of the instance within its own scene (alpha-blend hash key)
 };
 
 enum MatFlags : int { kMatAlbedoTex = 1, kMatEmissiveTex = 2, kMatNormalTex = 4, kMatMRTex = 8 };
@@ -118,6 +119,34 @@ struct WaveCounters {
     int pad[3];
 };
 
+// One render job of the shared wavefront (job engine): a scene, a camera and resolution, a
+// sample count and a trace depth, and its own accumulation buffers (3 floats per pixel;
+// comp only in the compensated form).
+struct DevJob {
+    int scene;
+    int width, height, npix;
+    int trace_depth;
+    int first_iter;       // iteration of the job's sample 0 (1-based, as the reference's iter)
+    uint32_t tlas_root;   // TLAS root of the job's scene in the concatenated node array
+    int pad;
+    float* image;
+    float* comp;
+    float pos[3], view[3], right[3], up[3];
+    float pixel_length[2];
+};
+
+// A wave segment: samples [sample0, sample0 + nsamples) of one job. Its paths occupy
+// [path0, path0 + nsamples * npix) sample-major; pix0 is the prefix of the wave's segment
+// pixel counts (the accumulate kernel's index space).
+struct DevSegment {
+    int job;
+    int sample0;
+    int nsamples;
+    int path0;
+    int pix0;
+};
+constexpr int kMaxSegments = 256;
+
 struct DevWave {
     float4* s0;
     float4* s1;
@@ -137,6 +166,12 @@ struct DevWave {
     int* queue_alt;
     WaveCounters* ctr;
     int* wave_iter;   // [0] first iteration of the wave, [1] samples in the wave
+    // job engine only (null for a single-job context):
+    const DevScene* scenes;    // per resident scene: geometry of the concatenated arrays + its lights
+    const DevJob* jobs;
+    const DevSegment* segs;    // the wave's segments, wave_hdr[0] of them
+    int* wave_hdr;             // [0] segments, [1] paths, [2] pixels over the segments
+    int* path_job;             // job of each path
     int npix;         // pixels of the job
     int width, height;
     int max_paths;

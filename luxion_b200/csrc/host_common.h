@@ -1,0 +1,166 @@
+// host_common.h -- host-side pieces shared by the single-job context (context.cpp) and the
+// job engine (engine.cpp): error reporting, device allocation, textures and the host-side
+// scene build with its upload.
+#pragma once
+
+#include "../../include/luxion.h"
+#include "bvh8.h"
+#include "device_scene.h"
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace lux {
+
+extern thread_local std::string g_err;
+// record msg for lux_last_error() and return code
+int fail(int code, const std::string& msg);
+
+#define LUX_CUDA(call)                                                                      \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess) {                                                            \
+            return ::lux::fail(e_ == cudaErrorMemoryAllocation ? LUX_ERR_OOM : LUX_ERR_CUDA, \
+                               std::string(#call) + ": " + cudaGetErrorString(e_));         \
+        }                                                                                   \
+    } while (0)
+
+template <class T>
+int dalloc(T** p, size_t n) {
+    *p = nullptr;
+    if (n == 0) return LUX_OK;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(T));
+    if (e != cudaSuccess) return fail(LUX_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    return LUX_OK;
+}
+template <class T>
+int upload(T** p, const T* src, size_t n) {
+    int rc = dalloc(p, n);
+    if (rc) return rc;
+    if (n) LUX_CUDA(cudaMemcpy(*p, src, n * sizeof(T), cudaMemcpyHostToDevice));
+    return LUX_OK;
+}
+
+struct DevTex {
+    cudaArray_t arr = nullptr;
+    cudaTextureObject_t obj = 0;
+    size_t bytes = 0;
+};
+inline void destroy_texture(DevTex& t) {
+    if (t.obj) cudaDestroyTextureObject(t.obj);
+    if (t.arr) cudaFreeArray(t.arr);
+    t = DevTex{};
+}
+
+// Everything a resident scene needs, built on the host (textures are created on the device
+// here because materials hold their texture objects): per-mesh BLASes concatenated, the
+// TLAS appended after them, instances, materials and the light tables.
+struct HostScene {
+    std::vector<BVH8Node> nodes;
+    uint32_t tlas_root = 0;           // first TLAS node; nodes from here on are the TLAS
+    std::vector<float4> prims;
+    std::vector<DevInstance> insts;
+    std::vector<uint32_t> tlas_prims;
+    std::vector<float> pos, nrm, uv;
+    std::vector<uint32_t> idx;
+    bool any_n = false, any_uv = false;
+    std::vector<DevMaterial> mats;
+    std::vector<int> emissive;        // emissive instances
+    std::vector<float> emissive_prefix, tri_prefix, marginal, conditional;
+    std::vector<int> tri_off;
+    float total_area = 0.0f;
+    int env_w = 0, env_h = 0;
+    unsigned long long env_tex = 0;
+    bool has_env = false;
+    float morton_bmin[3] = {0, 0, 0}, morton_bmax[3] = {0, 0, 0};
+    int64_t instanced_tris = 0;
+};
+
+// Check a scene description (sizes, index ranges, references, environment format).
+int validate_scene_desc(const lux_scene_desc& d);
+
+// Build of one validated scene description with the given options (texture storage,
+// precision, which light tables -dmis / -emis require). Textures are appended to texs; the
+// environment map goes to env.
+int build_host_scene(const lux_scene_desc& d, const lux_options& opt, std::vector<DevTex>& texs, DevTex& env,
+                     HostScene& H);
+
+// Upload the light tables of a host scene and set its environment and Morton box fields.
+// Owner provides up(T** dst, const T* src, size_t n), which records the allocation.
+template <class Owner>
+int upload_scene_lights(Owner* C, const HostScene& H, DevScene& S) {
+    int rc;
+    float* f = nullptr;
+    int* ei = nullptr;
+    if ((rc = C->up(&ei, H.emissive.data(), H.emissive.size()))) return rc;
+    S.emissive_inst = ei;
+    if ((rc = C->up(&f, H.emissive_prefix.data(), H.emissive_prefix.size()))) return rc;
+    S.emissive_prefix = f;
+    if ((rc = C->up(&f, H.tri_prefix.data(), H.tri_prefix.size()))) return rc;
+    S.tri_prefix = f;
+    if ((rc = C->up(&ei, H.tri_off.data(), H.tri_off.size()))) return rc;
+    S.tri_prefix_off = ei;
+    S.num_emissive = int(H.emissive.size());
+    S.total_area = H.total_area;
+    if (H.has_env) {
+        if ((rc = C->up(&f, H.marginal.data(), H.marginal.size()))) return rc;
+        S.marginal = f;
+        if ((rc = C->up(&f, H.conditional.data(), H.conditional.size()))) return rc;
+        S.conditional = f;
+        S.env_w = H.env_w;
+        S.env_h = H.env_h;
+        S.env_tex = H.env_tex;
+        S.has_env = 1;
+    }
+    for (int a = 0; a < 3; ++a) {
+        S.morton_bmin[a] = H.morton_bmin[a];
+        S.morton_bmax[a] = H.morton_bmax[a];
+    }
+    return LUX_OK;
+}
+
+// Upload a host scene (geometry, materials, then its light tables). Empty arrays upload as
+// null pointers.
+template <class Owner>
+int upload_scene(Owner* C, const HostScene& H, DevScene& S) {
+    std::memset(&S, 0, sizeof(S));
+    int rc;
+    uint4* dn = nullptr;
+    if ((rc = C->up(&dn, reinterpret_cast<const uint4*>(H.nodes.data()), H.nodes.size() * 5))) return rc;
+    S.nodes = dn;
+    float4* dp = nullptr;
+    if ((rc = C->up(&dp, H.prims.data(), H.prims.size()))) return rc;
+    S.prims = dp;
+    DevInstance* di = nullptr;
+    if ((rc = C->up(&di, H.insts.data(), H.insts.size()))) return rc;
+    S.insts = di;
+    uint32_t* dt = nullptr;
+    if ((rc = C->up(&dt, H.tlas_prims.data(), H.tlas_prims.size()))) return rc;
+    S.tlas_prims = dt;
+    S.tlas_root = H.tlas_root;
+    S.num_insts = int(H.insts.size());
+    float* f = nullptr;
+    if ((rc = C->up(&f, H.pos.data(), H.pos.size()))) return rc;
+    S.pos = f;
+    if (H.any_n) {
+        if ((rc = C->up(&f, H.nrm.data(), H.nrm.size()))) return rc;
+        S.nrm = f;
+    }
+    if (H.any_uv) {
+        if ((rc = C->up(&f, H.uv.data(), H.uv.size()))) return rc;
+        S.uv = f;
+    }
+    uint32_t* du = nullptr;
+    if ((rc = C->up(&du, H.idx.data(), H.idx.size()))) return rc;
+    S.idx = du;
+    DevMaterial* dm = nullptr;
+    if ((rc = C->up(&dm, H.mats.data(), H.mats.size()))) return rc;
+    S.mats = dm;
+    return upload_scene_lights(C, H, S);
+}
+
+}  // namespace lux

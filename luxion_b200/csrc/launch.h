@@ -14,7 +14,9 @@ int shade_grid_blocks();
 
 // persistent trace of bounce `bounce`: mode 0 radiance (queues shadow rays when nee != 0:
 // 1 DL, 2 env), 1 DL shadow rays, 2 env occlusion rays
-cudaError_t launch_trace(const DevScene& S, const DevWave& W, int bounce, int mode, int nee, cudaStream_t st);
+// grid > 0 overrides the persistent grid (blocks), for the job engine's autotuner
+cudaError_t launch_trace(const DevScene& S, const DevWave& W, int bounce, int mode, int nee, cudaStream_t st,
+                         int grid = 0);
 // trace caller rays (device buffers), n * 8 floats -> n * 5 words; fetch is a zeroed int
 cudaError_t launch_trace_ext(const DevScene& S, const DevWave& W, const float* rays, uint32_t* hits, int n, int mode,
                              int iter, int* fetch, cudaStream_t st);
@@ -35,6 +37,10 @@ cudaError_t launch_camera(const DevScene& S, const DevWave& W, const DevOptions&
 // shade bounce `bounce` (depth = bounce + 1 after the increment of src/pathtrace.cu:264)
 cudaError_t launch_shade(const DevScene& S, const DevWave& W, const DevOptions& O, int bounce, int compact,
                          cudaStream_t st);
+// job engine: camera rays of the wave's segments (counts read from W.wave_hdr), and the
+// per-job accumulation of the segments in sample order
+cudaError_t launch_camera_jobs(const DevWave& W, const DevOptions& O, int max_paths, cudaStream_t st);
+cudaError_t launch_accumulate_jobs(const DevWave& W, int compensated, cudaStream_t st);
 // image[p] (+comp) += radiance of every sample of the wave, in sample order
 cudaError_t launch_accumulate(const DevWave& W, float* image, float* comp, int nsamples, int compensated,
                               cudaStream_t st);

@@ -588,7 +588,11 @@ __global__ void __launch_bounds__(kShadeBlock) k_camera(DevScene S, DevWave W, D
     if (blockIdx.x == 0 && threadIdx.x == 0) W.ctr->count[0] = n;
 }
 
-__global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene S, DevWave W, DevOptions O, int bounce, int compact) {
+// JOBS: the shared wavefront of the job engine; each path shades against its job's scene
+// (lights, environment) and stops compacting at its job's trace depth.
+template <bool JOBS>
+__global__ void __launch_bounds__(kShadeBlock) k_shade(const __grid_constant__ DevScene S0, DevWave W, DevOptions O,
+                                                       int bounce, int compact) {
     const int n = *(volatile int*)&W.ctr->count[bounce];
     const int depth = bounce + 1;
     const int* q = W.queue[bounce & 1];
@@ -603,6 +607,14 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene S, DevWave W, De
         int pid = 0;
         if (slot < n) {
             pid = q[slot];
+            int job_compact = compact;
+            const DevScene* sp = &S0;
+            if (JOBS) {
+                const DevJob& J = W.jobs[W.path_job[pid]];
+                sp = &W.scenes[J.scene];
+                job_compact = depth < J.trace_depth;
+            }
+            const DevScene& S = *sp;
             PathState p = load_path(W, pid);
             float4 h = W.hit[slot];
             int inst = __float_as_int(h.w);
@@ -619,7 +631,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene S, DevWave W, De
                     spr = W.sh_prim[slot];
                 }
             }
-            alive = shade_one(S, O, depth, p, h.x, inst, prim, h.y, h.z, sh_t, si, spr, su, sv) && compact;
+            alive = shade_one(S, O, depth, p, h.x, inst, prim, h.y, h.z, sh_t, si, spr, su, sv) && job_compact;
             W.s3[pid] = make_float4(p.color.x, p.color.y, p.color.z, __int_as_float(p.iter));
             if (alive) {
                 W.s0[pid] = make_float4(p.o.x, p.o.y, p.o.z, p.last_pdf);
@@ -678,6 +690,105 @@ __global__ void k_accumulate(const float4* __restrict__ s3, float* __restrict__ 
         image[p * 3] = r;
         image[p * 3 + 1] = g;
         image[p * 3 + 2] = b;
+    }
+}
+
+// Segment of the wave holding index v of a prefix array (path0 or pix0), by binary search
+// over the segment table staged in shared memory.
+template <int FIELD>
+LUX_DI int find_segment(const DevSegment* segs, int nsegs, int v) {
+    int lo = 0, hi = nsegs - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        int start = FIELD == 0 ? segs[mid].path0 : segs[mid].pix0;
+        if (start <= v) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Camera rays of a job-engine wave (generateRayFromCamera, src/kernels/generate_ray_from_camera.cu:8-39,
+// per job): path pid belongs to the segment covering it; its sample s and pixel index give the
+// job-local iteration and pixel that seed the RNG, exactly as a single-job render would.
+__global__ void __launch_bounds__(kShadeBlock) k_camera_jobs(DevWave W, DevOptions O) {
+    __shared__ DevSegment segs[kMaxSegments];
+    const int nsegs = W.wave_hdr[0], n = W.wave_hdr[1];
+    for (int k = threadIdx.x; k < nsegs; k += blockDim.x) segs[k] = W.segs[k];
+    __syncthreads();
+    const bool nee = O.dl || O.env;
+    for (int pid = blockIdx.x * blockDim.x + threadIdx.x; pid < n; pid += gridDim.x * blockDim.x) {
+        const DevSegment& g = segs[find_segment<0>(segs, nsegs, pid)];
+        const DevJob& J = W.jobs[g.job];
+        int off = pid - g.path0;
+        int s = off / J.npix, index = off - s * J.npix;
+        int iter = J.first_iter + g.sample0 + s;
+        int x = index % J.width, y = index / J.width;
+        Rng rng = Rng::seeded(iter, index, J.trace_depth);
+        float x1 = rng.u01() - 0.5f;
+        float x2 = rng.u01() - 0.5f;
+        float pX = (float(x) + x1 + 0.5f) - float(J.width) * 0.5f;
+        float pY = (float(y) + x2 + 0.5f) - float(J.height) * 0.5f;
+        f3 view = ld3(J.view), right = ld3(J.right), up = ld3(J.up);
+        f3 d = normalize(view - (right * J.pixel_length[0] * pX) - (up * J.pixel_length[1] * pY));
+        W.s0[pid] = make_float4(J.pos[0], J.pos[1], J.pos[2], -1.0f);
+        W.s1[pid] = make_float4(d.x, d.y, d.z, __int_as_float(0));
+        W.s2[pid] = make_float4(1.0f, 1.0f, 1.0f, __int_as_float(index));
+        W.s3[pid] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(iter));
+        if (nee) {
+            f3 ed;
+            f3 dl = light_sample(W.scenes[J.scene], O, iter, index, 0, ed);
+            f3 v = O.env ? ed : dl;
+            W.s4[pid] = make_float4(v.x, v.y, v.z, 0.0f);
+        }
+        W.path_job[pid] = g.job;
+        W.queue[0][pid] = pid;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) W.ctr->count[0] = n;
+}
+
+// image[job pixel] (+comp) += radiance of the segment's samples, in sample order, so that a
+// job's image is the same bit for bit however its samples were split into waves.
+__global__ void k_accumulate_jobs(DevWave W, int compensated) {
+    __shared__ DevSegment segs[kMaxSegments];
+    const int nsegs = W.wave_hdr[0], total = W.wave_hdr[2];
+    for (int k = threadIdx.x; k < nsegs; k += blockDim.x) segs[k] = W.segs[k];
+    __syncthreads();
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += gridDim.x * blockDim.x) {
+        const DevSegment& g = segs[find_segment<1>(segs, nsegs, q)];
+        const DevJob& J = W.jobs[g.job];
+        const int p = q - g.pix0;
+        const size_t o = size_t(p) * 3;
+        float* __restrict__ image = J.image;
+        float* __restrict__ comp = J.comp;
+        float r = image[o], gr = image[o + 1], b = image[o + 2];
+        if (compensated) {
+            float cr = comp[o], cg = comp[o + 1], cb = comp[o + 2];
+            for (int s = 0; s < g.nsamples; ++s) {
+                float4 c = W.s3[size_t(g.path0) + size_t(s) * J.npix + p];
+                float yr = c.x - cr, tr = r + yr;
+                cr = (tr - r) - yr;
+                r = tr;
+                float yg = c.y - cg, tg = gr + yg;
+                cg = (tg - gr) - yg;
+                gr = tg;
+                float yb = c.z - cb, tb = b + yb;
+                cb = (tb - b) - yb;
+                b = tb;
+            }
+            comp[o] = cr;
+            comp[o + 1] = cg;
+            comp[o + 2] = cb;
+        } else {
+            for (int s = 0; s < g.nsamples; ++s) {
+                float4 c = W.s3[size_t(g.path0) + size_t(s) * J.npix + p];
+                r += c.x;
+                gr += c.y;
+                b += c.z;
+            }
+        }
+        image[o] = r;
+        image[o + 1] = gr;
+        image[o + 2] = b;
     }
 }
 
@@ -794,7 +905,10 @@ int shade_grid_blocks() {
         int dev = 0, sms = 0, per = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_shade, kShadeBlock, 0);
+        int per_jobs = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_shade<false>, kShadeBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_jobs, k_shade<true>, kShadeBlock, 0);
+        per = std::min(per, per_jobs);
         cached = sms * (per > 0 ? per : 1);
     }
     return cached;
@@ -810,7 +924,20 @@ cudaError_t launch_camera(const DevScene& S, const DevWave& W, const DevOptions&
 
 cudaError_t launch_shade(const DevScene& S, const DevWave& W, const DevOptions& O, int bounce, int compact,
                          cudaStream_t st) {
-    k_shade<<<shade_grid_blocks(), kShadeBlock, 0, st>>>(S, W, O, bounce, compact);
+    if (W.path_job) k_shade<true><<<shade_grid_blocks(), kShadeBlock, 0, st>>>(S, W, O, bounce, compact);
+    else k_shade<false><<<shade_grid_blocks(), kShadeBlock, 0, st>>>(S, W, O, bounce, compact);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_camera_jobs(const DevWave& W, const DevOptions& O, int max_paths, cudaStream_t st) {
+    int grid = std::min((max_paths + kShadeBlock - 1) / kShadeBlock, shade_grid_blocks() * 2);
+    if (grid < 1) grid = 1;
+    k_camera_jobs<<<grid, kShadeBlock, 0, st>>>(W, O);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_accumulate_jobs(const DevWave& W, int compensated, cudaStream_t st) {
+    k_accumulate_jobs<<<148 * 8, 256, 0, st>>>(W, compensated);
     return cudaGetLastError();
 }
 

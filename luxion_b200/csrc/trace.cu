@@ -182,7 +182,7 @@ LUX_DI bool alpha_accept(const DevScene& S, const DevInstance& I, int inst, int 
     h = hash_u32(h ^ __float_as_uint(wdir.x));
     h = hash_u32(h ^ __float_as_uint(wdir.y));
     h = hash_u32(h ^ __float_as_uint(wdir.z));
-    h = hash_u32(h ^ uint32_t(inst));
+    h = hash_u32(h ^ uint32_t(I.key));  // the instance's index within its own scene
     h = hash_u32(h ^ uint32_t(prim));
     float rnd = float(h >> 8) * (1.0f / 16777216.0f);
     return !(rnd >= alpha);
@@ -227,7 +227,7 @@ struct Tracer {
         return L.sp < kShStack ? sh[L.sp][tid] : loc[L.sp - kShStack];
     }
 
-    LUX_DI void start(Lane& L, f3 o, f3 d, float tmax) {
+    LUX_DI void start(Lane& L, f3 o, f3 d, float tmax, uint32_t root) {
         L.wo = o;
         L.wd = d;
         L.cur = make_ray(o, d);
@@ -242,7 +242,7 @@ struct Tracer {
         L.inst_prim_base = 0;
         L.done = false;
         // root group: a single internal child (slot 0) = the TLAS root, at key oct
-        L.g = make_uint2(S.tlas_root, (1u << 8) | (1u << L.cur.oct));
+        L.g = make_uint2(root, (1u << 8) | (1u << L.cur.oct));
         L.t = make_uint2(0u, 0u);
     }
 
@@ -415,6 +415,7 @@ __global__ void __launch_bounds__(kTraceBlock, 6) k_trace(const __grid_constant_
                     item = r;
                     f3 o, d;
                     float tmax;
+                    uint32_t root = A.S.tlas_root;
                     L.pixel = 0;
                     L.iter = 0;
                     if (ext) {
@@ -432,6 +433,7 @@ __global__ void __launch_bounds__(kTraceBlock, 6) k_trace(const __grid_constant_
                         tmax = 1e16f;
                         L.pixel = __float_as_int(A.W.s2[pid].w);
                         L.iter = __float_as_int(A.W.s3[pid].w);
+                        if (A.W.path_job) root = A.W.jobs[A.W.path_job[pid]].tlas_root;
                     } else {
                         int slot = A.W.sh_queue[r];
                         item = slot;
@@ -442,8 +444,9 @@ __global__ void __launch_bounds__(kTraceBlock, 6) k_trace(const __grid_constant_
                         int pid = A.W.queue[A.bounce & 1][slot];
                         L.pixel = __float_as_int(A.W.s2[pid].w);
                         L.iter = __float_as_int(A.W.s3[pid].w);
+                        if (A.W.path_job) root = A.W.jobs[A.W.path_job[pid]].tlas_root;
                     }
-                    T.start(L, o, d, tmax);
+                    T.start(L, o, d, tmax, root);
                     active = true;
                 }
             }
@@ -558,9 +561,10 @@ int trace_grid_blocks(int mode) {
     return cached[mode];
 }
 
-cudaError_t launch_trace(const DevScene& S, const DevWave& W, int bounce, int mode, int nee, cudaStream_t st) {
+cudaError_t launch_trace(const DevScene& S, const DevWave& W, int bounce, int mode, int nee, cudaStream_t st,
+                         int grid) {
     TraceArgs A{S, W, bounce, mode, nee, nullptr, nullptr, 0, 0, nullptr};
-    int grid = trace_grid_blocks(mode);
+    if (grid <= 0) grid = trace_grid_blocks(mode);
     if (mode == 0) k_trace<0><<<grid, kTraceBlock, 0, st>>>(A);
     else if (mode == 1) k_trace<1><<<grid, kTraceBlock, 0, st>>>(A);
     else k_trace<2><<<grid, kTraceBlock, 0, st>>>(A);

@@ -40,7 +40,9 @@ STRUCTS = {
     "lux_material_desc": _ffi.MaterialDesc, "lux_mesh_desc": _ffi.MeshDesc,
     "lux_instance_desc": _ffi.InstanceDesc, "lux_camera_desc": _ffi.CameraDesc,
     "lux_scene_desc": _ffi.SceneDesc, "lux_options": _ffi.Options, "lux_stats": _ffi.Stats,
-    "lux_random_scene_params": _ffi.RandomSceneParams,
+    "lux_random_scene_params": _ffi.RandomSceneParams, "lux_job_desc": _ffi.JobDesc,
+    "lux_engine_config": _ffi.EngineConfig, "lux_job_status": _ffi.JobStatus,
+    "lux_engine_stats": _ffi.EngineStats,
 }
 
 
