@@ -16,7 +16,15 @@ Reported (one JSON line, rank 0):
               beside it
   cpu_baseline  the reference's own render-path sources built for the host (oracle/_ref),
               OpenMP over pixel rows, on a bounded crop of the same workload
-With --impl reference only that CPU arm runs (rank 0).
+  batched     (one GPU) the batching form: 64 seeded jobs over 8 resident scenes of 10k-2M
+              triangles, mixed resolutions / spp / depths, rendered in one shared wavefront by the
+              job engine, against the same 64 jobs rendered one after another by single-job
+              contexts (render time alone, and with each job's lux_init); images compared bitwise
+  served      (one GPU) the serving form: Poisson requests at 50/s against 16 resident scenes
+              of 50k-4M triangles (binary16 HDRIs) under a 150 GB HBM budget, continuous batching
+              in the engine, against first-come-first-served single-job contexts; p50/p95/p99
+              latency and throughput of both
+With --impl reference only that CPU arm runs (rank 0). --no-forms skips batched and served.
 Under torchrun every rank renders its own 16 samples (disjoint iterations, weak scaling) and
 the FP32 images are summed with one NCCL all-reduce per step.
 """
@@ -51,6 +59,93 @@ def peaks():
             d = json.load(f)
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def run_batched(seed: int = 0):
+    """The batching form: 64 jobs in the job engine versus 64 sequential single-job renders."""
+    import luxion_b200 as lx
+    from luxion_b200 import workloads
+    from luxion_b200._ffi import default_options
+    t0 = time.perf_counter()
+    scenes, tris = workloads.batch_scenes(seed)
+    jobs = workloads.batch_jobs(len(scenes), seed=seed)
+    t_gen = time.perf_counter() - t0
+    opt = default_options(direct_light_sampling=1, env_importance_sampling=1)
+    t0 = time.perf_counter()
+    E = lx.Engine(scenes, opt)
+    t_create = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    ids = [E.submit(j["scene"], j["spp"], trace_depth=j["depth"], camera=j["camera"]) for j in jobs]
+    E.run()
+    t_batch = time.perf_counter() - t0
+    st = E.stats()
+    imgs = [E.image(i) for i in ids]
+    E.close()
+    samples = sum(j["camera"].width * j["camera"].height * j["spp"] for j in jobs)
+    t_init = t_render = 0.0
+    rays_plain = 0.0
+    same = 0
+    for j, img in zip(jobs, imgs):
+        sc = scenes[j["scene"]]
+        d = sc.desc
+        saved = type(d.camera).from_buffer_copy(d.camera)
+        d.camera = j["camera"]
+        t0 = time.perf_counter()
+        try:
+            r = lx.Renderer(sc, default_options(direct_light_sampling=1, env_importance_sampling=1,
+                                                trace_depth=j["depth"]))
+        finally:
+            d.camera = saved
+        t1 = time.perf_counter()
+        r.render(1, j["spp"])
+        ref = r.image_sum()
+        t2 = time.perf_counter()
+        rs = r.stats()
+        rays_plain += rs["rays_radiance"] + rs["rays_shadow"]
+        r.close()
+        t_init += t1 - t0
+        t_render += t2 - t1
+        same += int(np.array_equal(ref.view(np.uint32), img.view(np.uint32)))
+    for sc in scenes:
+        sc.close()
+    return {"workload": "64 jobs over 8 seeded scenes of %d-%d tris; res {128^2,256^2,512^2,1024^2,1920x1080}, "
+                        "spp {1,4,16,64}, depth 4..16, -dmis -emis" % (min(tris), max(tris)),
+            "samples": samples, "batched_s": t_batch, "batched_samples_per_s": samples / t_batch,
+            "batched_mrays_per_s": st["rays"] / t_batch / 1e6, "waves": st["waves"],
+            "autotuned": {"max_paths": st["max_paths"], "trace_blocks": st["trace_blocks"]},
+            "plain_render_s": t_render, "plain_samples_per_s": samples / t_render,
+            "plain_mrays_per_s": rays_plain / t_render / 1e6, "plain_init_s": t_init,
+            "speedup_vs_plain_render": t_render / t_batch, "speedup_vs_plain_with_init": (t_render + t_init) / t_batch,
+            "identical_images": f"{same}/{len(jobs)}", "engine_create_s": t_create, "scene_gen_s": t_gen,
+            "timing": "host wall clock around lux_engine_run (every wave ends in a stream sync) and around each "
+                      "plain lux_render + lux_copy_image"}
+
+
+def run_served(seed: int = 0, requests: int = 32, rate: float = 50.0):
+    """The serving form: continuous batching in the job engine versus FCFS single-job contexts."""
+    import luxion_b200 as lx
+    from luxion_b200 import serving, workloads
+    from luxion_b200._ffi import SCHED_SHORTEST_FIRST, default_options
+    scenes, tris = workloads.serving_scenes(seed)
+    reqs = workloads.request_stream(len(scenes), requests, rate, seed=seed)
+    opt = default_options(direct_light_sampling=1, env_importance_sampling=1)
+    E = lx.Engine(scenes, opt, hbm_budget_bytes=150 * 10**9, schedule=SCHED_SHORTEST_FIRST)
+    eng = serving.serve_engine(E, reqs, keep_images=True)
+    E.close()
+    plain = serving.serve_plain(scenes, reqs, default_options(direct_light_sampling=1, env_importance_sampling=1),
+                                keep_images=True)
+    same = sum(int(np.array_equal(eng["images"][i].view(np.uint32), plain["images"][i].view(np.uint32)))
+               for i in range(len(reqs)))
+    for sc in scenes:
+        sc.close()
+    eng.pop("images")
+    plain.pop("images")
+    return {"workload": "%d Poisson requests at %g/s over 16 seeded scenes of %d-%d tris (binary16 2048x1024 HDRI); "
+                        "log-normal res 256^2..1920x1080, spp 4..256, depth 12, random camera azimuth, -dmis -emis, "
+                        "150 GB HBM budget" % (requests, rate, min(tris), max(tris)),
+            "engine": eng, "plain_fcfs": plain, "identical_images": f"{same}/{len(reqs)}",
+            "p99_ratio_plain_over_engine": plain["p99_ms"] / eng["p99_ms"],
+            "throughput_ratio": eng["samples_per_s"] / plain["samples_per_s"]}
 
 
 def make_scene():
@@ -183,6 +278,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-forms", action="store_true")
+    ap.add_argument("--forms-only", action="store_true", help="run only the batched and served forms")
+    ap.add_argument("--serve-requests", type=int, default=32)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -191,6 +289,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
+        return
+    if args.forms_only:
+        print(json.dumps({"batched": run_batched(), "served": run_served(requests=args.serve_requests)}), flush=True)
         return
 
     import torch
@@ -323,6 +424,10 @@ def main():
         arm.calibrate(15.0)
         mr, sps, info = arm.measure()
         cpu = dict(info, value=mr, unit="Mrays/s", samples_per_s=sps)
+    batched = served = None
+    if rank == 0 and world == 1 and not args.no_forms:
+        batched = run_batched()
+        served = run_served(requests=args.serve_requests)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -338,7 +443,7 @@ def main():
             "samples_per_s": (W * H * SPP * world) / (t_all * 1e-3),
             "roofline": roof, "roofline_shade": roof_shade, "kernel_ms_one_step": breakdown,
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "gpu_launches": launches,
-            "served": None}
+            "batched": batched, "served": served}
     print(json.dumps(line), flush=True)
 
 

@@ -403,6 +403,12 @@ lux_host_scene* lux_scene_random(const lux_random_scene_params* p);
 /* Furnace: a closed unit sphere (Lambert albedo 1) inside a constant environment of 1. */
 lux_host_scene* lux_scene_furnace(int width, int height, int subdiv);
 
+/* A pinhole camera at pos looking at look (world up +y) with vertical field of view fovy_deg
+ * at width x height, set up as the reference's scene loader does from a camera's position,
+ * look-at point and fov: pixelLength = 2 tan(fovy/2) (aspect, 1) / resolution. */
+void lux_make_camera(int width, int height, const float pos[3], const float look[3], float fovy_deg,
+                     lux_camera_desc* out);
+
 const lux_scene_desc* lux_scene_get_desc(const lux_host_scene* s);
 /* Total triangles over all instances. */
 int64_t lux_scene_instanced_tris(const lux_host_scene* s);

@@ -65,6 +65,7 @@ SIGNATURES = {
     "lux_engine_clock_ms": (C.c_double, [_P]),
     "lux_engine_free": (C.c_int, [_P]),
     "lux_plan_wave": (C.c_int, [c_int_p, c_int_p, C.c_int, C.c_int, C.c_int, c_int_p]),
+    "lux_make_camera": (None, [C.c_int, C.c_int, c_float_p, c_float_p, C.c_float, C.POINTER(CameraDesc)]),
     "lux_scene_cornell36": (_P, [C.c_int, C.c_int]),
     "lux_default_random_scene_params": (None, [C.POINTER(RandomSceneParams)]),
     "lux_scene_random": (_P, [C.POINTER(RandomSceneParams)]),
@@ -355,6 +356,15 @@ class Engine:
             self.close()
         except Exception:
             pass
+
+
+def make_camera(width: int, height: int, pos, look, fovy_deg: float = 45.0) -> CameraDesc:
+    """A pinhole camera (lux_make_camera) at pos looking at look, world up +y."""
+    p = (C.c_float * 3)(*[float(x) for x in pos])
+    q = (C.c_float * 3)(*[float(x) for x in look])
+    cam = CameraDesc()
+    lib().lux_make_camera(width, height, p, q, float(fovy_deg), C.byref(cam))
+    return cam
 
 
 def plan_wave(npix, remaining, capacity: int, max_segments: int = 256) -> np.ndarray:

@@ -514,6 +514,14 @@ void make_sky(lux_host_scene& s, int W, int H, uint64_t seed, bool half) {
 
 extern "C" {
 
+void lux_make_camera(int width, int height, const float pos[3], const float look[3], float fovy_deg,
+                     lux_camera_desc* out) {
+    if (!out || !pos || !look) return;
+    const double p[3] = {pos[0], pos[1], pos[2]}, l[3] = {look[0], look[1], look[2]};
+    std::memset(out, 0, sizeof(*out));
+    set_camera(*out, width, height, p, l, fovy_deg);
+}
+
 lux_host_scene* lux_scene_cornell36(int width, int height) {
     auto s = std::make_unique<lux_host_scene>();
     std::memset(&s->desc, 0, sizeof(s->desc));

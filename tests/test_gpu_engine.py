@@ -135,3 +135,19 @@ def test_engine_argument_errors(scenes):
         E.release(j + 5)
     E.step()
     E.close()
+
+
+def test_serving_loop_latencies_and_images(scenes):
+    from luxion_b200 import serving, workloads
+    sc = [scenes["a"], scenes["b"]]
+    reqs = workloads.request_stream(2, 8, 200.0, seed=4, depth=5)
+    for r in reqs:       # small frames for a quick test
+        r["camera"] = lx.make_camera(40, 24, r["camera"].position[:], workloads.CAMERA_LOOK, 45.0)
+        r["spp"] = 1 + r["spp"] % 5
+    E = lx.Engine(sc, default_options(**OPT), max_paths=4000, schedule=_ffi.SCHED_SHORTEST_FIRST)
+    eng = serving.serve_engine(E, reqs, keep_images=True)
+    E.close()
+    plain = serving.serve_plain(sc, reqs, default_options(**OPT), keep_images=True)
+    assert eng["requests"] == 8 and eng["p50_ms"] <= eng["p99_ms"] and eng["p50_ms"] > 0
+    for i in range(8):
+        assert same(eng["images"][i], plain["images"][i]), i
