@@ -24,7 +24,10 @@ Reported (one JSON line, rank 0):
               of 50k-4M triangles (binary16 HDRIs) under a 150 GB HBM budget, continuous batching
               in the engine, against first-come-first-served single-job contexts; p50/p95/p99
               latency and throughput of both
-With --impl reference only that CPU arm runs (rank 0). --no-forms skips batched and served.
+  precision   (one GPU) the precision form (4M triangles, binary16 textures and HDRI, FP64 CDFs,
+              compensated accumulation, 1080p at 1024 spp) against the plain FP32 path on the
+              same scene and RNG streams: throughput of both and the relative difference
+With --impl reference only that CPU arm runs (rank 0). --no-forms skips batched, served, precision.
 Under torchrun every rank renders its own 16 samples (disjoint iterations, weak scaling) and
 the FP32 images are summed with one NCCL all-reduce per step.
 """
@@ -146,6 +149,39 @@ def run_served(seed: int = 0, requests: int = 32, rate: float = 50.0):
             "engine": eng, "plain_fcfs": plain, "identical_images": f"{same}/{len(reqs)}",
             "p99_ratio_plain_over_engine": plain["p99_ms"] / eng["p99_ms"],
             "throughput_ratio": eng["samples_per_s"] / plain["samples_per_s"]}
+
+
+def run_precision(spp: int = 1024):
+    """The precision form on its own workload (the 1M-triangle generator scaled to 4M triangles,
+    binary16 textures and HDRI, FP64 light CDFs, compensated accumulation, 1920x1080 at 1024 spp)
+    against the plain FP32 path on the same scene and samples. Both use the same RNG streams, so
+    the difference of their images is the arithmetic and storage error, without sampling noise."""
+    import luxion_b200 as lx
+    from luxion_b200 import _ffi
+    from luxion_b200._ffi import default_options
+    sc = lx.random_scene(seed=0, total_tris=4_000_000, num_instances=200, min_tris=5000, max_tris=80000,
+                         tex_half=1, env_half=1)
+    out = {"workload": "4M tris / 200 instances, 1920x1080, %d spp, depth 12, -dmis -emis, seed 0" % spp}
+    imgs = {}
+    for name, opt in (("precision", default_options(direct_light_sampling=1, env_importance_sampling=1,
+                                                    precision=_ffi.PRECISION_COMPENSATED,
+                                                    texture_storage=_ffi.TEXSTORE_HALF)),
+                      ("plain_fp32", default_options(direct_light_sampling=1, env_importance_sampling=1))):
+        r = lx.Renderer(sc, opt)
+        r.render(1, 4)      # warm-up: graph capture
+        r.reset()
+        r.render(1, spp)
+        st = r.stats()
+        imgs[name] = r.image_sum().astype(np.float64)
+        r.close()
+        out[name] = {"ms": st["ms_total"], "samples_per_s": st["samples"] / (st["ms_total"] * 1e-3),
+                     "mrays_per_s": (st["rays_radiance"] + st["rays_shadow"]) / (st["ms_total"] * 1e-3) / 1e6}
+    a, b = imgs["precision"], imgs["plain_fp32"]
+    out["relmse_precision_vs_plain"] = float(np.mean((a - b) ** 2) / np.mean(b ** 2))
+    out["mean_rel_diff"] = float(np.mean(np.abs(a - b)) / np.mean(np.abs(b)))
+    out["instanced_tris"] = sc.instanced_tris
+    sc.close()
+    return out
 
 
 def make_scene():
@@ -291,7 +327,8 @@ def main():
         run_reference_arm(args, rank, world)
         return
     if args.forms_only:
-        print(json.dumps({"batched": run_batched(), "served": run_served(requests=args.serve_requests)}), flush=True)
+        print(json.dumps({"precision": run_precision(), "batched": run_batched(),
+                          "served": run_served(requests=args.serve_requests)}), flush=True)
         return
 
     import torch
@@ -424,10 +461,11 @@ def main():
         arm.calibrate(15.0)
         mr, sps, info = arm.measure()
         cpu = dict(info, value=mr, unit="Mrays/s", samples_per_s=sps)
-    batched = served = None
+    batched = served = precision = None
     if rank == 0 and world == 1 and not args.no_forms:
         batched = run_batched()
         served = run_served(requests=args.serve_requests)
+        precision = run_precision()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -443,7 +481,7 @@ def main():
             "samples_per_s": (W * H * SPP * world) / (t_all * 1e-3),
             "roofline": roof, "roofline_shade": roof_shade, "kernel_ms_one_step": breakdown,
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "gpu_launches": launches,
-            "batched": batched, "served": served}
+            "batched": batched, "served": served, "precision": precision}
     print(json.dumps(line), flush=True)
 
 
