@@ -67,6 +67,10 @@ struct DevScene {
     const float4* prims;
     const DevInstance* insts;
     const uint32_t* tlas_prims;  // TLAS leaf records -> instance index
+    // per TLAS leaf record, what entering its instance needs in one 64-byte load: the
+    // world -> object matrix (12 floats, as DevInstance::Minv) in three float4, then
+    // (blas_root, prim_base, flags, instance) as int bits
+    const float4* tlas_leaf;
     uint32_t tlas_root;
     int num_insts;
     const float* pos;

@@ -141,6 +141,19 @@ int upload_scene(Owner* C, const HostScene& H, DevScene& S) {
     uint32_t* dt = nullptr;
     if ((rc = C->up(&dt, H.tlas_prims.data(), H.tlas_prims.size()))) return rc;
     S.tlas_prims = dt;
+    std::vector<float4> leaf(H.tlas_prims.size() * 4);
+    for (size_t k = 0; k < H.tlas_prims.size(); ++k) {
+        const DevInstance& I = H.insts[H.tlas_prims[k]];
+        float4* q = &leaf[k * 4];
+        q[0] = make_float4(I.Minv[0], I.Minv[1], I.Minv[2], I.Minv[3]);
+        q[1] = make_float4(I.Minv[4], I.Minv[5], I.Minv[6], I.Minv[7]);
+        q[2] = make_float4(I.Minv[8], I.Minv[9], I.Minv[10], I.Minv[11]);
+        const uint32_t e[4] = {I.blas_root, I.prim_base, uint32_t(I.flags), H.tlas_prims[k]};
+        std::memcpy(&q[3], e, 16);
+    }
+    float4* dl = nullptr;
+    if ((rc = C->up(&dl, leaf.data(), leaf.size()))) return rc;
+    S.tlas_leaf = dl;
     S.tlas_root = H.tlas_root;
     S.num_insts = int(H.insts.size());
     float* f = nullptr;

@@ -64,7 +64,8 @@ LUX_DI TRay make_ray(f3 o, f3 d) {
     return r;
 }
 
-LUX_DI float ubyte(uint32_t w, int s) { return __uint_as_float(0x4B000000u | ((w >> (8 * s)) & 0xffu)) - 8388608.0f; }
+// byte s of w as a float: one byte permute builds 0x4B0000bb (2^23 + byte), one add removes 2^23
+LUX_DI float ubyte(uint32_t w, int s) { return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u | uint32_t(s))) - 8388608.0f; }
 
 // Intersect the 8 child boxes of node ni. Returns internal-child hits as a key mask
 // (bit (slot ^ oct)), the leaf primitive mask (bit offset), child_base and tri_base.
@@ -294,16 +295,19 @@ struct Tracer {
         uint32_t m = L.t.y & kRecMask;
         int k = __ffs(m) - 1;
         m &= m - 1;
-        int ii = int(__ldg(S.tlas_prims + L.t.x + uint32_t(k)));
+        // the instance's leaf record: transform and BLAS root in one dependent 64-byte load
+        const float4* q = S.tlas_leaf + size_t(L.t.x + uint32_t(k)) * 4;
+        const float4 r0 = __ldg(q), r1 = __ldg(q + 1), r2 = __ldg(q + 2);
+        const uint4 e = __ldg(reinterpret_cast<const uint4*>(q + 3));
         if (L.g.y & 0xffu) push(L, L.g);
         if (m) push(L, make_uint2(L.t.x, kTagInst | m));
         push(L, make_uint2(0u, kTagMarker));
-        const DevInstance& I = S.insts[ii];
-        L.cur = make_ray(xform(I.Minv, L.wo, 1.0f), xform(I.Minv, L.wd, 0.0f));
-        L.inst = ii;
-        L.inst_flags = I.flags;
-        L.inst_prim_base = I.prim_base;
-        L.g = make_uint2(I.blas_root, (1u << 8) | (1u << L.cur.oct));
+        const float Minv[12] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w};
+        L.cur = make_ray(xform(Minv, L.wo, 1.0f), xform(Minv, L.wd, 0.0f));
+        L.inst = int(e.w);
+        L.inst_flags = int(e.z);
+        L.inst_prim_base = e.y;
+        L.g = make_uint2(e.x, (1u << 8) | (1u << L.cur.oct));
         L.t = make_uint2(0u, 0u);
     }
 
