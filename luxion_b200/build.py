@@ -9,6 +9,7 @@ Translation units:
               rounded on its own, in the reference's order
   sort.cu     Morton keys and the radix sort of a bounce queue
   trace_static.cu  the fixed device scratch of lux_trace_rays_static
+  texconv.cu  texel conversion (8/16-bit to float or binary16) at scene upload
   context.cpp, engine.cpp, bvh_build.cpp, scene_gen.cpp   host C++ (no FMA contraction)
 The CUDA runtime is linked statically so the library does not depend on which libcudart a
 host process (for example PyTorch) has already loaded.
@@ -36,6 +37,7 @@ CU_UNITS = {
     "shade.cu": ["--fmad=false"],
     "sort.cu": ["--fmad=true"],
     "trace_static.cu": ["--fmad=true"],
+    "texconv.cu": ["--fmad=false"],
 }
 CPP_UNITS = ["context.cpp", "engine.cpp", "bvh_build.cpp", "scene_gen.cpp"]
 

@@ -138,35 +138,34 @@ float half_bits_to_float(uint16_t h) {
 }
 
 // Upload one texture. storage LUX_TEXSTORE_FLOAT converts 8/16-bit unorm texels to float4 as
-// TextureHandler::load_textures_on_device does (c/255, c/65535; src/texture.cu:12-69),
+// TextureHandler::load_textures_on_device does (c/255, c/65535; src/texture.cu:12-69; on the
+// device, texconv.cu),
 // LUX_TEXSTORE_HALF converts them to binary16, LUX_TEXSTORE_UNORM8 keeps 8-bit texels (16-bit
 // ones become float4). Binary16 texels stay binary16 under every storage.
 int make_texture(const lux_texture_desc& t, DevTex& out, int storage) {
     if (t.width <= 0 || t.height <= 0 || !t.data) return fail(LUX_ERR_INVALID, "empty texture");
     const size_t n = size_t(t.width) * t.height * 4;
-    std::vector<float> f32;
-    std::vector<__half> f16;
     const void* src = t.data;
     int fmt = t.format;
-    auto to_float = [&](size_t i) -> float {
-        switch (t.format) {
-            case LUX_TEX_RGBA8: return float(static_cast<const uint8_t*>(t.data)[i]) / 255.0f;
-            case LUX_TEX_RGBA16: return float(static_cast<const uint16_t*>(t.data)[i]) / 65535.0f;
-            case LUX_TEX_RGBA16F: return half_bits_to_float(static_cast<const uint16_t*>(t.data)[i]);
-            default: return static_cast<const float*>(t.data)[i];
+    // conversions run on the device: the texels are uploaded as they are and converted there
+    const bool to_half = storage == LUX_TEXSTORE_HALF && t.format != LUX_TEX_RGBA16F;
+    const bool to_float = (storage == LUX_TEXSTORE_FLOAT && t.format == LUX_TEX_RGBA8) ||
+                          (storage != LUX_TEXSTORE_HALF && t.format == LUX_TEX_RGBA16);
+    struct DevBuf {
+        void* p = nullptr;
+        ~DevBuf() {
+            if (p) cudaFree(p);
         }
-    };
-    if (storage == LUX_TEXSTORE_HALF && t.format != LUX_TEX_RGBA16F) {
-        f16.resize(n);
-        for (size_t i = 0; i < n; ++i) f16[i] = __float2half_rn(to_float(i));
-        src = f16.data();
-        fmt = LUX_TEX_RGBA16F;
-    } else if ((storage == LUX_TEXSTORE_FLOAT && t.format == LUX_TEX_RGBA8) ||
-               (storage != LUX_TEXSTORE_HALF && t.format == LUX_TEX_RGBA16)) {
-        f32.resize(n);
-        for (size_t i = 0; i < n; ++i) f32[i] = to_float(i);
-        src = f32.data();
-        fmt = LUX_TEX_RGBA32F;
+    } dsrc, ddst;
+    const void* dev_src = nullptr;
+    if (to_half || to_float) {
+        const size_t in_bytes = t.format == LUX_TEX_RGBA8 ? 1 : (t.format == LUX_TEX_RGBA32F ? 4 : 2);
+        LUX_CUDA(cudaMalloc(&dsrc.p, n * in_bytes));
+        LUX_CUDA(cudaMalloc(&ddst.p, n * (to_half ? 2 : 4)));
+        LUX_CUDA(cudaMemcpy(dsrc.p, t.data, n * in_bytes, cudaMemcpyHostToDevice));
+        LUX_CUDA(launch_convert_texels(dsrc.p, t.format, to_half ? 1 : 0, ddst.p, n, 0));
+        dev_src = ddst.p;
+        fmt = to_half ? LUX_TEX_RGBA16F : LUX_TEX_RGBA32F;
     }
     cudaChannelFormatDesc fd;
     size_t texel;
@@ -194,8 +193,12 @@ int make_texture(const lux_texture_desc& t, DevTex& out, int storage) {
             return fail(LUX_ERR_INVALID, "unknown texture format");
     }
     LUX_CUDA(cudaMallocArray(&out.arr, &fd, t.width, t.height));
-    LUX_CUDA(cudaMemcpy2DToArray(out.arr, 0, 0, src, size_t(t.width) * texel, size_t(t.width) * texel, t.height,
-                                 cudaMemcpyHostToDevice));
+    if (dev_src)
+        LUX_CUDA(cudaMemcpy2DToArray(out.arr, 0, 0, dev_src, size_t(t.width) * texel, size_t(t.width) * texel,
+                                     t.height, cudaMemcpyDeviceToDevice));
+    else
+        LUX_CUDA(cudaMemcpy2DToArray(out.arr, 0, 0, src, size_t(t.width) * texel, size_t(t.width) * texel, t.height,
+                                     cudaMemcpyHostToDevice));
     out.bytes = size_t(t.width) * t.height * texel;
     cudaResourceDesc rd{};
     rd.resType = cudaResourceTypeArray;
@@ -323,10 +326,16 @@ int lux::build_host_scene(const lux_scene_desc& d, const lux_options& opt, std::
     const int NM = d.num_meshes;
     std::vector<BVH8Build> blas(NM);
     {
+        // largest meshes first, so that no large build starts last on an otherwise idle pool
+        std::vector<int> by_size(NM);
+        for (int m = 0; m < NM; ++m) by_size[m] = m;
+        std::stable_sort(by_size.begin(), by_size.end(),
+                         [&](int a, int b) { return d.meshes[a].num_tris > d.meshes[b].num_tris; });
         std::atomic<int> next{0};
         unsigned nt = std::max(1u, std::min(std::thread::hardware_concurrency(), 64u));
         auto work = [&]() {
-            for (int m = next++; m < NM; m = next++) {
+            for (int k = next++; k < NM; k = next++) {
+                const int m = by_size[k];
                 const lux_mesh_desc& md = d.meshes[m];
                 std::vector<float> boxes(size_t(md.num_tris) * 6);
                 for (int k = 0; k < md.num_tris; ++k) {

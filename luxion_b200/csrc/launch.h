@@ -46,6 +46,10 @@ cudaError_t launch_accumulate(const DevWave& W, float* image, float* comp, int n
                               cudaStream_t st);
 cudaError_t launch_tonemap(const float* image, uint8_t* rgba, int npix, float iter, int color_mode, cudaStream_t st);
 
+// n texel channels at src (device) of format fmt (LUX_TEX_RGBA8/16/32F) to float (c / 255,
+// c / 65535) or, with to_half, to binary16 at dst (device); texconv.cu
+cudaError_t launch_convert_texels(const void* src, int fmt, int to_half, void* dst, size_t n, cudaStream_t st);
+
 // Morton keys of the bounce's queue and a stable LSD radix sort of the queue by key
 cudaError_t launch_morton_sort(const DevScene& S, DevWave& W, int bounce, void* temp, size_t temp_bytes,
                                cudaStream_t st);
