@@ -371,9 +371,10 @@ def main():
             e0.record(stream)
             step(args.warmup + k)
             if world > 1:
-                # combine the ranks' sample sums (the one collective of the sharded path)
-                img = torch.from_numpy(r.image_sum().reshape(-1)).cuda()
-                dist.all_reduce(img)
+                # combine the ranks' sample sums (the one collective of the sharded path),
+                # device to device: copy into a torch tensor on the same stream, all-reduce
+                r.copy_image_device(img_dev.data_ptr())
+                dist.all_reduce(img_dev)
             e1.record(stream)
             e1.synchronize()
             ms.append(e0.elapsed_time(e1))

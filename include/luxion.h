@@ -186,6 +186,10 @@ int lux_render(lux_ctx* ctx, int first_iter, int n_iter);
 
 /* copyImageToHost: the accumulation SUM (not the mean), W*H*3 floats. */
 int lux_copy_image(lux_ctx* ctx, float* rgb_host);
+/* The same sum copied to device memory of the context's device (rgb_dev: W*H*3 floats), on
+ * the context's stream and without waiting for it: for combining the images of several GPUs
+ * with a device collective. */
+int lux_copy_image_device(lux_ctx* ctx, float* rgb_dev);
 
 /* Tonemapped RGBA8 of the running mean into a host buffer (W*H*4 bytes). */
 int lux_copy_rgba8(lux_ctx* ctx, uint8_t* rgba_host);

@@ -45,6 +45,7 @@ SIGNATURES = {
     "lux_enable_timing": (C.c_int, [_P, C.c_int]),
     "lux_get_stats": (C.c_int, [_P, C.POINTER(Stats)]),
     "lux_wave_counts": (C.c_int, [_P, c_int_p, c_int_p, C.c_int]),
+    "lux_copy_image_device": (C.c_int, [_P, C.c_void_p]),
     "lux_trace_rays": (C.c_int, [_P, c_float_p, C.c_int, C.c_int, C.c_int, c_u32_p]),
     "lux_trace_rays_static": (C.c_int, [_P, c_float_p, C.c_int, C.c_int, C.c_int, c_u32_p]),
     "lux_morton_keys": (C.c_int, [_P, c_float_p, C.c_int, c_u32_p]),
@@ -209,6 +210,11 @@ class Renderer:
         s = Stats()
         _check(lib().lux_get_stats(self._h, C.byref(s)))
         return {n: getattr(s, n) for n, _ in Stats._fields_}
+
+    def copy_image_device(self, dev_ptr: int):
+        """Copy the accumulation sum (W*H*3 floats) to device memory at dev_ptr, on the
+        context's stream, without waiting."""
+        _check(lib().lux_copy_image_device(self._h, C.c_void_p(dev_ptr)))
 
     def wave_counts(self, max_bounces: int = 64):
         """(paths entering each bounce, shadow rays per bounce) of the last wave rendered."""

@@ -925,6 +925,14 @@ int lux_copy_image(lux_ctx* C, float* rgb_host) {
     return LUX_OK;
 }
 
+int lux_copy_image_device(lux_ctx* C, float* rgb_dev) {
+    if (!C || !rgb_dev) return fail(LUX_ERR_INVALID, "NULL argument");
+    LUX_CUDA(cudaSetDevice(C->device));
+    LUX_CUDA(cudaMemcpyAsync(rgb_dev, C->image, size_t(C->npix) * 3 * sizeof(float), cudaMemcpyDeviceToDevice,
+                             C->stream));
+    return LUX_OK;
+}
+
 int lux_copy_rgba8(lux_ctx* C, uint8_t* rgba_host) {
     if (!C || !rgba_host) return fail(LUX_ERR_INVALID, "NULL argument");
     cudaSetDevice(C->device);

@@ -355,3 +355,17 @@ def test_option_validation_on_device():
     with pytest.raises(lx.LuxError) as e:
         lx.Renderer(sb, default_options(direct_light_sampling=1))
     assert "emissive" in str(e.value)
+
+
+def test_copy_image_device_equals_host_copy():
+    """The device-to-device image copy the multi-GPU bench all-reduces from."""
+    import torch
+    s = lx.cornell36(32, 32)
+    stream = torch.cuda.current_stream()
+    r = lx.Renderer(s, default_options(direct_light_sampling=1, stream=stream.cuda_stream))
+    r.render(1, 3)
+    dev = torch.zeros(32 * 32 * 3, dtype=torch.float32, device="cuda")
+    r.copy_image_device(dev.data_ptr())
+    stream.synchronize()
+    assert np.array_equal(dev.cpu().numpy().view(np.uint32), r.image_sum().reshape(-1).view(np.uint32))
+    r.close()
