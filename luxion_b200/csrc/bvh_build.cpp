@@ -6,8 +6,8 @@
 // 15% median fallback, :278-294, is replaced by an object-median split when binning cannot
 // separate the centroids). Leaves hold one primitive.
 // Collapse stage: each 8-wide node takes its binary node's two children and repeatedly opens
-// the child of largest surface area until 8 slots are used; subtrees of at most 3
-// primitives become leaf slots. Slots are assigned by child-centroid octant, boxes are
+// the child of largest surface area until 8 slots are used; subtrees of at most
+// kMaxLeafPrims primitives become leaf slots. Slots are assigned by child-centroid octant, boxes are
 // quantised outward.
 
 #include "bvh8.h"
