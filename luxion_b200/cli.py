@@ -3,10 +3,11 @@
     python -m luxion_b200 SCENE [-e|--envmap ENVMAP] [-i|--iterations N] [-o|--output NAME]
                                 [-dmis] [-emis] [-lock]
 
-SCENE is a procedural scene: cornell (the 36-triangle Cornell box), random[:SEED[:TRIS]] (the
-instanced test scene) or furnace; glTF files need the reference's scene loader, which this
-build does not include. ENVMAP is a float32 .npy array of HxWx3 or HxWx4 texels replacing the
-scene's environment map. -lock is accepted and ignored (it locks the interactive camera).
+SCENE is a glTF 2.0 file (.glb or .gltf, loaded as the reference's loader does: luxion_b200.gltf)
+or a procedural scene: cornell (the 36-triangle Cornell box), random[:SEED[:TRIS]] (the
+instanced test scene) or furnace. ENVMAP is an OpenEXR (.exr) or Radiance (.hdr) image, or a
+float32 .npy array of HxWx3 or HxWx4 texels, replacing the scene's environment map. -lock is
+accepted and ignored (it locks the interactive camera).
 The image is written as NAME.png the way the reference's saveImage does
 (src/app/save_image.cpp:42-84): the accumulated sum divided by the sample count, ACES, gamma
 0.45, x mirrored, each channel clamped to [0, 1] and truncated from value * 255.
@@ -22,8 +23,8 @@ from typing import List, Optional
 
 import numpy as np
 
-USAGE = ("Usage: %s SCENE [-e|--envmap ENVMAP] [-i|--iterations N] [-o|--output NAME] [-dmis] [-emis] [-lock]\n"
-         "  SCENE: cornell | random[:SEED[:TRIS]] | furnace")
+USAGE = ("Usage: %s SCENEFILE [-e|--envmap ENVMAP] [-i|--iterations N] [-o|--output NAME] [-dmis] [-emis] [-lock]\n"
+         "  SCENEFILE: a .glb/.gltf file, or cornell | random[:SEED[:TRIS]] | furnace")
 
 
 def parse_args(argv: List[str]) -> dict:
@@ -115,8 +116,35 @@ def read_png(path: str) -> np.ndarray:
     return raw[:, 1:].reshape(h, w, 3).copy()
 
 
+def load_envmap(path: str) -> np.ndarray:
+    """HxWx4 float32 RGBA texels of an .exr / .hdr image (alpha 1 where the file has none)
+    or of an .npy array."""
+    if path.lower().endswith(".npy"):
+        env = np.load(path).astype(np.float32)
+    else:
+        os.environ.setdefault("OPENCV_IO_ENABLE_OPENEXR", "1")
+        import cv2
+        env = cv2.imread(path, cv2.IMREAD_UNCHANGED)
+        if env is None:
+            raise ValueError(f"Error: cannot read environment map '{path}'")
+        env = env.astype(np.float32)
+        if env.ndim == 3 and env.shape[2] >= 3:   # OpenCV gives BGR(A)
+            env = np.concatenate([env[..., 2::-1], env[..., 3:]], axis=2)
+    if env.ndim != 3 or env.shape[2] not in (3, 4):
+        raise ValueError(f"Error: environment map '{path}' must have 3 or 4 channels")
+    if env.shape[2] == 3:
+        env = np.concatenate([env, np.ones(env.shape[:2] + (1,), np.float32)], axis=2)
+    return np.ascontiguousarray(env)
+
+
 def make_scene(spec: str):
     import luxion_b200 as lx
+    if spec.lower().endswith((".glb", ".gltf")):
+        from luxion_b200 import gltf
+        try:
+            return gltf.load(spec)
+        except (OSError, ValueError, KeyError) as e:
+            raise ValueError(f"Error: cannot load scene '{spec}': {e}")
     parts = spec.split(":")
     name = parts[0].lower()
     if name in ("cornell", "cornell36"):
@@ -130,8 +158,8 @@ def make_scene(spec: str):
         return lx.random_scene(**kw)
     if name == "furnace":
         return lx.furnace()
-    raise ValueError(f"Error: cannot load scene '{spec}': this build renders the procedural scenes cornell, "
-                     "random[:SEED[:TRIS]] and furnace (glTF loading is not included)")
+    raise ValueError(f"Error: cannot load scene '{spec}': give a .glb/.gltf file or one of the procedural "
+                     "scenes cornell, random[:SEED[:TRIS]], furnace")
 
 
 def main(argv: Optional[List[str]] = None) -> int:
@@ -150,13 +178,11 @@ def main(argv: Optional[List[str]] = None) -> int:
         return 1
     keep = None
     if a["envmap"]:
-        env = np.load(a["envmap"]).astype(np.float32)
-        if env.ndim != 3 or env.shape[2] not in (3, 4):
-            print(f"Error: environment map '{a['envmap']}' must be an HxWx3 or HxWx4 array")
+        try:
+            keep = env = load_envmap(a["envmap"])
+        except (OSError, ValueError) as e:
+            print(e)
             return 1
-        if env.shape[2] == 3:
-            env = np.concatenate([env, np.ones(env.shape[:2] + (1,), np.float32)], axis=2)
-        keep = np.ascontiguousarray(env)
         d = scene.desc
         d.env_width, d.env_height, d.env_format = env.shape[1], env.shape[0], _ffi.TEX_RGBA32F
         d.env_data = keep.ctypes.data

@@ -24,7 +24,7 @@ def test_flags_as_the_reference_parses_them():
     with pytest.raises(ValueError):
         cli.parse_args(["-dmis"])
     assert cli.main([]) == 1
-    assert cli.main(["scene.glb"]) == 1      # glTF loading is not part of this build
+    assert cli.main(["missing.glb"]) == 1    # a scene file that cannot be read
 
 
 def test_save_image_rule():
@@ -50,3 +50,17 @@ def test_png_round_trip():
         p = os.path.join(d, "t.png")
         cli.write_png(p, rgb)
         assert np.array_equal(cli.read_png(p), rgb)
+
+
+def test_envmap_readers_give_rgba():
+    os.environ.setdefault("OPENCV_IO_ENABLE_OPENEXR", "1")  # before OpenCV is imported
+    import cv2
+    env = (np.random.default_rng(1).random((6, 10, 3)) * 20).astype(np.float32)
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "e.exr")
+        assert cv2.imwrite(p, env[..., ::-1])      # OpenCV writes BGR
+        got = cli.load_envmap(p)
+        assert got.shape == (6, 10, 4) and np.array_equal(got[..., :3], env) and np.all(got[..., 3] == 1)
+        q = os.path.join(d, "e.npy")
+        np.save(q, env)
+        assert np.array_equal(cli.load_envmap(q)[..., :3], env)
