@@ -56,13 +56,31 @@ struct Binary {
 
 constexpr int kBins = 32;
 
+// One primitive of the binary build: its box, its centroid and its index, kept in a packed
+// array that is partitioned in place, so every pass over a node's range reads memory in order.
+struct PrimRec {
+    float lo[3], hi[3], c[3];
+    uint32_t id;
+};
+
+int bin_of(float c, float lo, double k1) {
+    int b = int((double(c) - lo) * k1);
+    return std::min(kBins - 1, std::max(0, b));
+}
+
 void build_binary(const float* boxes, int n, Binary& B) {
     B.nodes.clear();
     B.order.resize(n);
-    for (int i = 0; i < n; ++i) B.order[i] = uint32_t(i);
-    std::vector<float> cen(size_t(n) * 3);
-    for (int i = 0; i < n; ++i)
-        for (int a = 0; a < 3; ++a) cen[size_t(i) * 3 + a] = 0.5f * (boxes[i * 6 + a] + boxes[i * 6 + 3 + a]);
+    std::vector<PrimRec> rec(static_cast<size_t>(n));
+    for (int i = 0; i < n; ++i) {
+        PrimRec& r = rec[size_t(i)];
+        for (int a = 0; a < 3; ++a) {
+            r.lo[a] = boxes[size_t(i) * 6 + a];
+            r.hi[a] = boxes[size_t(i) * 6 + 3 + a];
+            r.c[a] = 0.5f * (r.lo[a] + r.hi[a]);
+        }
+        r.id = uint32_t(i);
+    }
     B.nodes.reserve(size_t(2 * n));
     B.nodes.push_back(BNode());
     B.nodes[0].begin = 0;
@@ -72,72 +90,118 @@ void build_binary(const float* boxes, int n, Binary& B) {
         int ni = work.back();
         work.pop_back();
         BNode nd = B.nodes[ni];
+        PrimRec* r0 = rec.data() + nd.begin;
+        PrimRec* r1 = r0 + nd.count;
         Box cb;
-        for (int k = nd.begin; k < nd.begin + nd.count; ++k) {
-            uint32_t p = B.order[k];
-            Box pb;
-            std::memcpy(pb.lo, &boxes[size_t(p) * 6], 12);
-            std::memcpy(pb.hi, &boxes[size_t(p) * 6 + 3], 12);
-            nd.box.grow(pb);
-            cb.grow(&cen[size_t(p) * 3]);
+        for (const PrimRec* r = r0; r < r1; ++r) {
+            for (int a = 0; a < 3; ++a) {
+                nd.box.lo[a] = std::min(nd.box.lo[a], r->lo[a]);
+                nd.box.hi[a] = std::max(nd.box.hi[a], r->hi[a]);
+            }
+            cb.grow(r->c);
         }
         if (nd.count <= 1) {
             B.nodes[ni] = nd;
             continue;
         }
+        if (nd.count == 2) {
+            // Two primitives land in the first and last bins of every axis their centroids
+            // span, every such split costs the same, and the first axis wins: the smaller
+            // centroid on it goes left. Coincident centroids split the range in half.
+            for (int a = 0; a < 3; ++a) {
+                if (!(double(cb.hi[a]) - double(cb.lo[a]) > 0.0)) continue;
+                if (r0[1].c[a] < r0[0].c[a]) std::swap(r0[0], r0[1]);
+                break;
+            }
+            int l = int(B.nodes.size());
+            B.nodes.push_back(BNode());
+            B.nodes.push_back(BNode());
+            nd.left = l;
+            nd.right = l + 1;
+            B.nodes[l].begin = nd.begin;
+            B.nodes[l].count = 1;
+            B.nodes[l + 1].begin = nd.begin + 1;
+            B.nodes[l + 1].count = 1;
+            B.nodes[ni] = nd;
+            work.push_back(l);
+            work.push_back(l + 1);
+            continue;
+        }
+        // Bin all three axes in one pass; an axis whose centroids coincide takes no part. A bin's
+        // box is written on its first primitive, and only non-empty bins enter the sweep: a run of
+        // empty bins leaves both sides of a split unchanged, so the split after the last non-empty
+        // bin on the left is the lowest-index one of equal cost.
+        bool live[3];
+        double k1[3];
+        for (int a = 0; a < 3; ++a) {
+            double ext = double(cb.hi[a]) - double(cb.lo[a]);
+            live[a] = ext > 0.0;
+            k1[a] = live[a] ? kBins / ext : 0.0;
+        }
+        struct BinBox {
+            float lo[3], hi[3];
+        };
+        BinBox bb[3][kBins];
+        int bc[3][kBins] = {};
+        for (const PrimRec* r = r0; r < r1; ++r) {
+            for (int a = 0; a < 3; ++a) {
+                if (!live[a]) continue;
+                int b = bin_of(r->c[a], cb.lo[a], k1[a]);
+                BinBox& x = bb[a][b];
+                if (bc[a][b]++ == 0) {
+                    for (int d = 0; d < 3; ++d) {
+                        x.lo[d] = r->lo[d];
+                        x.hi[d] = r->hi[d];
+                    }
+                } else {
+                    for (int d = 0; d < 3; ++d) {
+                        x.lo[d] = std::min(x.lo[d], r->lo[d]);
+                        x.hi[d] = std::max(x.hi[d], r->hi[d]);
+                    }
+                }
+            }
+        }
         int best_axis = -1, best_split = -1;
         double best_cost = DBL_MAX;
         for (int a = 0; a < 3; ++a) {
-            double ext = double(cb.hi[a]) - double(cb.lo[a]);
-            if (!(ext > 0.0)) continue;
-            Box bb[kBins];
-            int bc[kBins] = {0};
-            double k1 = kBins / ext;
-            for (int k = nd.begin; k < nd.begin + nd.count; ++k) {
-                uint32_t p = B.order[k];
-                int b = int((double(cen[size_t(p) * 3 + a]) - cb.lo[a]) * k1);
-                b = std::min(kBins - 1, std::max(0, b));
-                Box pb;
-                std::memcpy(pb.lo, &boxes[size_t(p) * 6], 12);
-                std::memcpy(pb.hi, &boxes[size_t(p) * 6 + 3], 12);
-                bb[b].grow(pb);
-                bc[b]++;
-            }
+            if (!live[a]) continue;
+            int nb = 0, idx[kBins];
+            for (int b = 0; b < kBins; ++b)
+                if (bc[a][b] != 0) idx[nb++] = b;
             double ra[kBins];
             int rc[kBins];
             Box acc;
             int cnt = 0;
-            for (int b = kBins - 1; b > 0; --b) {
-                acc.grow(bb[b]);
-                cnt += bc[b];
-                ra[b] = acc.area();
-                rc[b] = cnt;
+            for (int j = nb - 1; j > 0; --j) {
+                const BinBox& x = bb[a][idx[j]];
+                acc.grow(x.lo);
+                acc.grow(x.hi);
+                cnt += bc[a][idx[j]];
+                ra[j] = acc.area();
+                rc[j] = cnt;
             }
             Box lacc;
             int lcnt = 0;
-            for (int b = 0; b < kBins - 1; ++b) {
-                lacc.grow(bb[b]);
-                lcnt += bc[b];
-                if (lcnt == 0 || rc[b + 1] == 0) continue;
-                double c = lacc.area() * lcnt + ra[b + 1] * rc[b + 1];
+            for (int j = 0; j < nb - 1; ++j) {
+                const BinBox& x = bb[a][idx[j]];
+                lacc.grow(x.lo);
+                lacc.grow(x.hi);
+                lcnt += bc[a][idx[j]];
+                double c = lacc.area() * lcnt + ra[j + 1] * rc[j + 1];
                 if (c < best_cost) {
                     best_cost = c;
                     best_axis = a;
-                    best_split = b;
+                    best_split = idx[j];
                 }
             }
         }
         int mid;
         if (best_axis >= 0) {
-            int a = best_axis;
-            double ext = double(cb.hi[a]) - double(cb.lo[a]);
-            double k1 = kBins / ext;
-            auto it = std::partition(B.order.begin() + nd.begin, B.order.begin() + nd.begin + nd.count, [&](uint32_t p) {
-                int b = int((double(cen[size_t(p) * 3 + a]) - cb.lo[a]) * k1);
-                b = std::min(kBins - 1, std::max(0, b));
-                return b <= best_split;
-            });
-            mid = int(it - B.order.begin());
+            const int a = best_axis;
+            const float lo = cb.lo[a];
+            const double k = k1[a];
+            PrimRec* it = std::partition(r0, r1, [&](const PrimRec& r) { return bin_of(r.c[a], lo, k) <= best_split; });
+            mid = nd.begin + int(it - r0);
         } else {
             mid = nd.begin + nd.count / 2;  // coincident centroids: split the range in half
         }
@@ -155,6 +219,7 @@ void build_binary(const float* boxes, int n, Binary& B) {
         work.push_back(l);
         work.push_back(l + 1);
     }
+    for (int i = 0; i < n; ++i) B.order[size_t(i)] = rec[size_t(i)].id;
 }
 
 // Quantise the child boxes of one 8-wide node. The node box is first widened by a relative
@@ -228,60 +293,68 @@ void build_bvh8(const float* boxes, int n, BVH8Build& out) {
         out.depth = std::max(out.depth, it.level);
         const BNode& bn = B.nodes[it.bnode];
         // gather up to 8 children
-        std::vector<int> ch;
+        int ch[8];
+        int nch = 0;
         if (bn.left < 0 || bn.count <= kMaxLeafPrims) {
-            ch.push_back(it.bnode);  // the whole node is one leaf slot
+            ch[nch++] = it.bnode;  // the whole node is one leaf slot
         } else {
-            ch.push_back(bn.left);
-            ch.push_back(bn.right);
-            while (ch.size() < 8) {
+            ch[nch++] = bn.left;
+            ch[nch++] = bn.right;
+            while (nch < 8) {
                 int pick = -1;
                 double pa = -1.0;
-                for (size_t k = 0; k < ch.size(); ++k) {
+                for (int k = 0; k < nch; ++k) {
                     const BNode& c = B.nodes[ch[k]];
                     if (c.left < 0 || c.count <= kMaxLeafPrims) continue;
                     double a = c.box.area();
                     if (a > pa) {
                         pa = a;
-                        pick = int(k);
+                        pick = k;
                     }
                 }
                 if (pick < 0) break;
                 int c = ch[pick];
                 ch[pick] = B.nodes[c].left;
-                ch.push_back(B.nodes[c].right);
+                ch[nch++] = B.nodes[c].right;
             }
         }
-        // slot assignment by centroid octant around the node centre
+        // Slot assignment by centroid octant around the node centre: child c in slot s costs
+        // the centroid offset projected on the octant's direction; pairs are taken cheapest
+        // first (ties by child, then slot), skipping a pair whose child or slot is taken.
         float ctr[3];
         for (int a = 0; a < 3; ++a) ctr[a] = 0.5f * (bn.box.lo[a] + bn.box.hi[a]);
         int slot_of[8];
         bool slot_used[8] = {false};
         {
-            struct P {
-                double cost;
-                int c, s;
-            };
-            std::vector<P> ps;
-            for (size_t k = 0; k < ch.size(); ++k) {
+            double cost[8][8];
+            for (int k = 0; k < nch; ++k) {
                 const Box& b = B.nodes[ch[k]].box;
                 double d[3];
                 for (int a = 0; a < 3; ++a) d[a] = 0.5 * (double(b.lo[a]) + double(b.hi[a])) - ctr[a];
                 for (int s = 0; s < 8; ++s) {
                     double c = 0;
                     for (int a = 0; a < 3; ++a) c += ((s >> a) & 1) ? -d[a] : d[a];
-                    ps.push_back({c, int(k), s});
+                    cost[k][s] = c;
                 }
             }
-            std::sort(ps.begin(), ps.end(), [](const P& x, const P& y) {
-                return x.cost < y.cost || (x.cost == y.cost && (x.c < y.c || (x.c == y.c && x.s < y.s)));
-            });
             bool cdone[8] = {false};
-            for (const P& p : ps) {
-                if (cdone[p.c] || slot_used[p.s]) continue;
-                cdone[p.c] = true;
-                slot_used[p.s] = true;
-                slot_of[p.c] = p.s;
+            for (int round = 0; round < nch; ++round) {
+                int bc = -1, bs = -1;
+                double bcost = 0.0;
+                for (int k = 0; k < nch; ++k) {
+                    if (cdone[k]) continue;
+                    for (int s = 0; s < 8; ++s) {
+                        if (slot_used[s]) continue;
+                        if (bc < 0 || cost[k][s] < bcost) {
+                            bcost = cost[k][s];
+                            bc = k;
+                            bs = s;
+                        }
+                    }
+                }
+                cdone[bc] = true;
+                slot_used[bs] = true;
+                slot_of[bc] = bs;
             }
         }
         BVH8Node N;
@@ -289,7 +362,7 @@ void build_bvh8(const float* boxes, int n, BVH8Build& out) {
         Box cbox[8];
         int child_at_slot[8];
         for (int s = 0; s < 8; ++s) child_at_slot[s] = -1;
-        for (size_t k = 0; k < ch.size(); ++k) {
+        for (int k = 0; k < nch; ++k) {
             child_at_slot[slot_of[k]] = ch[k];
             cbox[slot_of[k]] = B.nodes[ch[k]].box;
         }

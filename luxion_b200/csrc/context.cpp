@@ -213,21 +213,35 @@ int make_texture(const lux_texture_desc& t, DevTex& out, int storage) {
     return LUX_OK;
 }
 
-// Texel values as the reference holds them (float4) for the HDRI CDF build.
+// Run fn(lo, hi) over [0, n) split into contiguous chunks, one per host thread.
+template <class F>
+void parallel_chunks(int n, F fn) {
+    unsigned nt = std::max(1u, std::min(std::thread::hardware_concurrency(), 64u));
+    nt = std::max(1u, std::min(nt, unsigned((n + 63) / 64)));
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < nt; ++t) th.emplace_back(fn, int(int64_t(n) * t / nt), int(int64_t(n) * (t + 1) / nt));
+    fn(0, int(int64_t(n) / nt));
+    for (auto& t : th) t.join();
+}
+
 // The environment texels the HDRI CDF is built from: the values the env texture holds on the
 // device, so that with binary16 storage the importance-sampling tables follow the stored map.
-void env_texels(const lux_scene_desc& d, int storage, std::vector<float>& out) {
-    size_t n = size_t(d.env_width) * d.env_height * 4;
-    out.resize(n);
-    if (d.env_format == LUX_TEX_RGBA16F) {
-        const uint16_t* s = static_cast<const uint16_t*>(d.env_data);
-        for (size_t i = 0; i < n; ++i) out[i] = half_bits_to_float(s[i]);
-    } else {
-        const float* s = static_cast<const float*>(d.env_data);
-        std::copy(s, s + n, out.begin());
-        if (storage == LUX_TEXSTORE_HALF)
-            for (size_t i = 0; i < n; ++i) out[i] = __half2float(__float2half_rn(out[i]));
-    }
+// Returns the scene's own array when it already holds those values, else fills `tmp`.
+const float* env_texels(const lux_scene_desc& d, int storage, std::vector<float>& tmp) {
+    const size_t n = size_t(d.env_width) * d.env_height * 4;
+    if (d.env_format != LUX_TEX_RGBA16F && storage != LUX_TEXSTORE_HALF) return static_cast<const float*>(d.env_data);
+    tmp.resize(n);
+    const int rows = d.env_height;
+    const size_t row = size_t(d.env_width) * 4;
+    parallel_chunks(rows, [&](int y0, int y1) {
+        for (size_t i = size_t(y0) * row; i < size_t(y1) * row; ++i) {
+            if (d.env_format == LUX_TEX_RGBA16F)
+                tmp[i] = half_bits_to_float(static_cast<const uint16_t*>(d.env_data)[i]);
+            else
+                tmp[i] = __half2float(__float2half_rn(static_cast<const float*>(d.env_data)[i]));
+        }
+    });
+    return tmp.data();
 }
 
 // Emissive-area and HDRI CDFs as Scene::precompute_emissive_mesh_area and
@@ -235,7 +249,7 @@ void env_texels(const lux_scene_desc& d, int storage, std::vector<float>& out) {
 // prefix sums in T, then normalised. T = float reproduces the reference bit for bit; the
 // precision form uses T = double and rounds the final tables to float.
 template <class T>
-bool light_tables(const lux_scene_desc& d, const std::vector<float>& env, std::vector<int>& emissive,
+bool light_tables(const lux_scene_desc& d, const float* env, std::vector<int>& emissive,
                   std::vector<float>& eprefix, std::vector<std::vector<float>>& tri_prefix, float& total_area,
                   std::vector<float>& marginal, std::vector<float>& conditional) {
     const float kEPS = 0.00001f;
@@ -286,26 +300,33 @@ bool light_tables(const lux_scene_desc& d, const std::vector<float>& env, std::v
     if (!d.env_data) return true;
     const int W = d.env_width, H = d.env_height;
     const float kPI = 3.1415926535897932384626422832795028841971f;
-    std::vector<T> cond(size_t(W) * H), marg(H);
+    // rows are independent; only the row totals chain, in row order
+    std::vector<T> cond(size_t(W) * H), marg(H), rows(H);
+    parallel_chunks(H, [&](int y0, int y1) {
+        for (int y = y0; y < y1; ++y) {
+            T rt = T(0);
+            T theta = T(kPI) * (T(y) + T(0.5f)) / T(H);
+            T st = std::sin(theta);
+            T* cy = &cond[size_t(y) * W];
+            for (int x = 0; x < W; ++x) {
+                const float* p = &env[(size_t(y) * W + x) * 4];
+                T a = T(p[0]) * T(p[0]), b = T(p[1]) * T(p[1]), c = T(p[2]) * T(p[2]), dd = T(p[3]) * T(p[3]);
+                T e = std::sqrt((a + b) + (c + dd));
+                rt += e * st;
+                cy[x] = rt;
+            }
+            if (rt > T(0)) {
+                for (int x = 0; x < W; ++x) cy[x] /= rt;
+            } else {
+                for (int x = 0; x < W; ++x) cy[x] = T(x + 1) / T(W);
+            }
+            cy[W - 1] = T(1);
+            rows[y] = rt;
+        }
+    });
     T total = T(0);
     for (int y = 0; y < H; ++y) {
-        T rt = T(0);
-        T theta = T(kPI) * (T(y) + T(0.5f)) / T(H);
-        T st = std::sin(theta);
-        for (int x = 0; x < W; ++x) {
-            const float* p = &env[(size_t(y) * W + x) * 4];
-            T a = T(p[0]) * T(p[0]), b = T(p[1]) * T(p[1]), c = T(p[2]) * T(p[2]), dd = T(p[3]) * T(p[3]);
-            T e = std::sqrt((a + b) + (c + dd));
-            rt += e * st;
-            cond[size_t(y) * W + x] = rt;
-        }
-        if (rt > T(0)) {
-            for (int x = 0; x < W; ++x) cond[size_t(y) * W + x] /= rt;
-        } else {
-            for (int x = 0; x < W; ++x) cond[size_t(y) * W + x] = T(x + 1) / T(W);
-        }
-        cond[size_t(y) * W + (W - 1)] = T(1);
-        total += rt;
+        total += rows[y];
         marg[y] = total;
     }
     if (total == T(0)) return false;  // the reference exits: "HDRI has emission of 0.0f"
@@ -314,7 +335,9 @@ bool light_tables(const lux_scene_desc& d, const std::vector<float>& env, std::v
     marginal.resize(H);
     conditional.resize(size_t(W) * H);
     for (int y = 0; y < H; ++y) marginal[y] = float(marg[y]);
-    for (size_t k = 0; k < cond.size(); ++k) conditional[k] = float(cond[k]);
+    parallel_chunks(H, [&](int y0, int y1) {
+        for (size_t k = size_t(y0) * W; k < size_t(y1) * W; ++k) conditional[k] = float(cond[k]);
+    });
     return true;
 }
 
@@ -322,9 +345,56 @@ bool light_tables(const lux_scene_desc& d, const std::vector<float>& env, std::v
 
 int lux::build_host_scene(const lux_scene_desc& d, const lux_options& opt, std::vector<DevTex>& texs,
                           DevTex& env, HostScene& H) {
-    // ---- per-mesh BLAS (threaded across meshes) ----
     const int NM = d.num_meshes;
+    const int NI = d.num_instances;
+    // ---- textures and the environment map, on their own thread during the BLAS builds ----
+    const size_t tex0 = texs.size();
+    texs.resize(tex0 + d.num_textures);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int tex_rc = LUX_OK;
+    std::string tex_err;
+    std::thread texer([&]() {
+        if (cudaSetDevice(dev) != cudaSuccess) {
+            tex_rc = fail(LUX_ERR_CUDA, "cudaSetDevice failed on the texture thread");
+            tex_err = g_err;
+            return;
+        }
+        for (int t = 0; t < d.num_textures && tex_rc == LUX_OK; ++t)
+            tex_rc = make_texture(d.textures[t], texs[tex0 + t], opt.texture_storage);
+        if (tex_rc == LUX_OK && d.env_data) {
+            lux_texture_desc et{d.env_width, d.env_height, d.env_format, 0, d.env_data};
+            tex_rc = make_texture(et, env, opt.texture_storage == LUX_TEXSTORE_HALF ? LUX_TEXSTORE_HALF : LUX_TEXSTORE_FLOAT);
+        }
+        if (tex_rc) tex_err = g_err;
+    });
+    struct Joiner {
+        std::thread& t;
+        ~Joiner() {
+            if (t.joinable()) t.join();
+        }
+    } joiner{texer};
+
+    // ---- per-mesh BLAS, triangle records and vertex data (threaded across meshes) ----
+    // Triangle, vertex and index offsets follow from the counts; node offsets only from the
+    // finished builds, so nodes are concatenated afterwards.
+    bool& any_n = H.any_n;
+    bool& any_uv = H.any_uv;
+    std::vector<size_t> tri_off(size_t(NM) + 1, 0), vert_off(size_t(NM) + 1, 0);
+    for (int m = 0; m < NM; ++m) {
+        any_n |= d.meshes[m].normals != nullptr;
+        any_uv |= d.meshes[m].uvs != nullptr;
+        tri_off[m + 1] = tri_off[m] + size_t(d.meshes[m].num_tris);
+        vert_off[m + 1] = vert_off[m] + size_t(d.meshes[m].num_verts);
+    }
+    H.prims.resize(tri_off[NM] * 3);
+    H.idx.resize(tri_off[NM] * 3);
+    H.pos.resize(vert_off[NM] * 3);
+    if (any_n) H.nrm.resize(vert_off[NM] * 3);
+    if (any_uv) H.uv.resize(vert_off[NM] * 2);
     std::vector<BVH8Build> blas(NM);
+    std::vector<float> mesh_box(size_t(NM) * 6);
+    std::atomic<bool> bad_order{false};
     {
         // largest meshes first, so that no large build starts last on an otherwise idle pool
         std::vector<int> by_size(NM);
@@ -337,9 +407,10 @@ int lux::build_host_scene(const lux_scene_desc& d, const lux_options& opt, std::
             for (int k = next++; k < NM; k = next++) {
                 const int m = by_size[k];
                 const lux_mesh_desc& md = d.meshes[m];
-                std::vector<float> boxes(size_t(md.num_tris) * 6);
-                for (int k = 0; k < md.num_tris; ++k) {
-                    float* b = &boxes[size_t(k) * 6];
+                const size_t nv = size_t(md.num_verts), ntri = size_t(md.num_tris);
+                std::vector<float> boxes(ntri * 6);
+                for (size_t k = 0; k < ntri; ++k) {
+                    float* b = &boxes[k * 6];
                     for (int a = 0; a < 3; ++a) {
                         b[a] = FLT_MAX;
                         b[3 + a] = -FLT_MAX;
@@ -358,6 +429,45 @@ int lux::build_host_scene(const lux_scene_desc& d, const lux_options& opt, std::
                     }
                 }
                 build_bvh8(boxes.data(), md.num_tris, blas[m]);
+                if (blas[m].prim_order.size() != ntri) {
+                    bad_order = true;
+                    continue;
+                }
+                // triangle records in leaf order: v0 with the triangle index in w, e1, e2
+                float4* out = H.prims.data() + tri_off[m] * 3;
+                for (uint32_t p : blas[m].prim_order) {
+                    const float* v0 = md.positions + size_t(md.indices[p * 3]) * 3;
+                    const float* v1 = md.positions + size_t(md.indices[p * 3 + 1]) * 3;
+                    const float* v2 = md.positions + size_t(md.indices[p * 3 + 2]) * 3;
+                    float pf;
+                    int32_t pi = int32_t(p);
+                    std::memcpy(&pf, &pi, 4);
+                    *out++ = make_float4(v0[0], v0[1], v0[2], pf);
+                    *out++ = make_float4(v1[0] - v0[0], v1[1] - v0[1], v1[2] - v0[2], 0.0f);
+                    *out++ = make_float4(v2[0] - v0[0], v2[1] - v0[1], v2[2] - v0[2], 0.0f);
+                }
+                std::memcpy(H.idx.data() + tri_off[m] * 3, md.indices, ntri * 3 * sizeof(uint32_t));
+                std::memcpy(H.pos.data() + vert_off[m] * 3, md.positions, nv * 3 * sizeof(float));
+                if (any_n) {
+                    float* dst = H.nrm.data() + vert_off[m] * 3;
+                    if (md.normals) std::memcpy(dst, md.normals, nv * 3 * sizeof(float));
+                    else std::fill(dst, dst + nv * 3, 0.0f);
+                }
+                if (any_uv) {
+                    float* dst = H.uv.data() + vert_off[m] * 2;
+                    if (md.uvs) std::memcpy(dst, md.uvs, nv * 2 * sizeof(float));
+                    else std::fill(dst, dst + nv * 2, 0.0f);
+                }
+                float* b = &mesh_box[size_t(m) * 6];
+                for (int a = 0; a < 3; ++a) {
+                    b[a] = FLT_MAX;
+                    b[3 + a] = -FLT_MAX;
+                }
+                for (size_t v = 0; v < nv; ++v)
+                    for (int a = 0; a < 3; ++a) {
+                        b[a] = std::min(b[a], md.positions[v * 3 + a]);
+                        b[3 + a] = std::max(b[3 + a], md.positions[v * 3 + a]);
+                    }
             }
         };
         std::vector<std::thread> th;
@@ -365,69 +475,39 @@ int lux::build_host_scene(const lux_scene_desc& d, const lux_options& opt, std::
         work();
         for (auto& t : th) t.join();
     }
-    // ---- concatenate meshes ----
-    std::vector<BVH8Node>& nodes = H.nodes;
-    std::vector<float4>& prims = H.prims;
-    std::vector<float>&pos = H.pos, &nrm = H.nrm, &uv = H.uv;
-    std::vector<uint32_t>& idx = H.idx;
-    std::vector<uint32_t> mesh_root(NM), mesh_prim(NM), mesh_vert(NM), mesh_idx(NM);
-    std::vector<int> mesh_flags(NM);
-    std::vector<float> mesh_box(size_t(NM) * 6);
-    bool& any_n = H.any_n;
-    bool& any_uv = H.any_uv;
-    for (int m = 0; m < NM; ++m) {
-        any_n |= d.meshes[m].normals != nullptr;
-        any_uv |= d.meshes[m].uvs != nullptr;
-    }
+    if (bad_order) return fail(LUX_ERR_UNSUPPORTED, "BVH leaf order does not cover every triangle once");
+    // ---- concatenate the BLAS nodes ----
+    std::vector<size_t> node_off(size_t(NM) + 1, 0);
     int max_blas_depth = 0;
     for (int m = 0; m < NM; ++m) {
-        const lux_mesh_desc& md = d.meshes[m];
-        const BVH8Build& B = blas[m];
-        max_blas_depth = std::max(max_blas_depth, B.depth);
-        uint32_t nb = uint32_t(nodes.size());
-        mesh_root[m] = nb;
-        for (BVH8Node n : B.nodes) {
-            n.child_base += nb;
-            nodes.push_back(n);
-        }
-        mesh_prim[m] = uint32_t(prims.size() / 3);
-        for (uint32_t p : B.prim_order) {
-            const float* v0 = md.positions + size_t(md.indices[p * 3]) * 3;
-            const float* v1 = md.positions + size_t(md.indices[p * 3 + 1]) * 3;
-            const float* v2 = md.positions + size_t(md.indices[p * 3 + 2]) * 3;
-            float pf;
-            int32_t pi = int32_t(p);
-            std::memcpy(&pf, &pi, 4);
-            prims.push_back(make_float4(v0[0], v0[1], v0[2], pf));
-            prims.push_back(make_float4(v1[0] - v0[0], v1[1] - v0[1], v1[2] - v0[2], 0.0f));
-            prims.push_back(make_float4(v2[0] - v0[0], v2[1] - v0[1], v2[2] - v0[2], 0.0f));
-        }
-        mesh_vert[m] = uint32_t(pos.size() / 3);
-        mesh_idx[m] = uint32_t(idx.size() / 3);
-        pos.insert(pos.end(), md.positions, md.positions + size_t(md.num_verts) * 3);
-        if (any_n) {
-            if (md.normals) nrm.insert(nrm.end(), md.normals, md.normals + size_t(md.num_verts) * 3);
-            else nrm.insert(nrm.end(), size_t(md.num_verts) * 3, 0.0f);
-        }
-        if (any_uv) {
-            if (md.uvs) uv.insert(uv.end(), md.uvs, md.uvs + size_t(md.num_verts) * 2);
-            else uv.insert(uv.end(), size_t(md.num_verts) * 2, 0.0f);
-        }
-        idx.insert(idx.end(), md.indices, md.indices + size_t(md.num_tris) * 3);
-        mesh_flags[m] = (md.normals ? kInstHasNormals : 0) | (md.uvs ? kInstHasUVs : 0);
-        float* b = &mesh_box[size_t(m) * 6];
-        for (int a = 0; a < 3; ++a) {
-            b[a] = FLT_MAX;
-            b[3 + a] = -FLT_MAX;
-        }
-        for (int v = 0; v < md.num_verts; ++v)
-            for (int a = 0; a < 3; ++a) {
-                b[a] = std::min(b[a], md.positions[size_t(v) * 3 + a]);
-                b[3 + a] = std::max(b[3 + a], md.positions[size_t(v) * 3 + a]);
+        node_off[m + 1] = node_off[m] + blas[m].nodes.size();
+        max_blas_depth = std::max(max_blas_depth, blas[m].depth);
+    }
+    H.nodes.reserve(node_off[NM] + size_t(NI) + 8);  // room for the TLAS nodes appended below
+    H.nodes.resize(node_off[NM]);
+    parallel_chunks(NM, [&](int m0, int m1) {
+        for (int m = m0; m < m1; ++m) {
+            BVH8Node* dst = H.nodes.data() + node_off[m];
+            const uint32_t nb = uint32_t(node_off[m]);
+            for (const BVH8Node& n : blas[m].nodes) {
+                *dst = n;
+                dst->child_base += nb;
+                ++dst;
             }
+            std::vector<BVH8Node>().swap(blas[m].nodes);
+        }
+    });
+    std::vector<uint32_t> mesh_root(NM), mesh_prim(NM), mesh_vert(NM), mesh_idx(NM);
+    std::vector<int> mesh_flags(NM);
+    for (int m = 0; m < NM; ++m) {
+        const lux_mesh_desc& md = d.meshes[m];
+        mesh_root[m] = uint32_t(node_off[m]);
+        mesh_prim[m] = uint32_t(tri_off[m]);
+        mesh_vert[m] = uint32_t(vert_off[m]);
+        mesh_idx[m] = uint32_t(tri_off[m]);
+        mesh_flags[m] = (md.normals ? kInstHasNormals : 0) | (md.uvs ? kInstHasUVs : 0);
     }
     // ---- instances + TLAS ----
-    const int NI = d.num_instances;
     std::vector<DevInstance>& insts = H.insts;
     insts.assign(NI, DevInstance{});
     std::vector<float> iboxes(size_t(NI) * 6);
@@ -489,22 +569,18 @@ int lux::build_host_scene(const lux_scene_desc& d, const lux_options& opt, std::
     }
     BVH8Build tl;
     build_bvh8(iboxes.data(), NI, tl);
-    uint32_t tlas_root = uint32_t(nodes.size());
+    uint32_t tlas_root = uint32_t(H.nodes.size());
     H.tlas_root = tlas_root;
     for (BVH8Node n : tl.nodes) {
         n.child_base += tlas_root;
-        nodes.push_back(n);
+        H.nodes.push_back(n);
     }
     H.tlas_prims.assign(tl.prim_order.begin(), tl.prim_order.end());
     if (tl.depth + max_blas_depth + 4 > 16 + 48)
         return fail(LUX_ERR_UNSUPPORTED, "acceleration structure deeper than the traversal stack");
     // ---- materials + textures ----
-    const size_t tex0 = texs.size();
-    texs.resize(tex0 + d.num_textures);
-    for (int t = 0; t < d.num_textures; ++t) {
-        int rc = make_texture(d.textures[t], texs[tex0 + t], opt.texture_storage);
-        if (rc) return rc;
-    }
+    texer.join();
+    if (tex_rc) return fail(tex_rc, tex_err);
     std::vector<DevMaterial>& mats = H.mats;
     mats.assign(d.num_materials, DevMaterial{});
     for (int k = 0; k < d.num_materials; ++k) {
@@ -547,8 +623,8 @@ int lux::build_host_scene(const lux_scene_desc& d, const lux_options& opt, std::
         tt(s.metallic_roughness_tt, m.mr_tt);
     }
     // ---- light tables ----
-    std::vector<float> envt;
-    if (d.env_data) env_texels(d, opt.texture_storage, envt);
+    std::vector<float> envt_tmp;
+    const float* envt = d.env_data ? env_texels(d, opt.texture_storage, envt_tmp) : nullptr;
     std::vector<std::vector<float>> tri_prefix;
     bool env_ok;
     if (opt.precision == LUX_PRECISION_COMPENSATED)
@@ -569,9 +645,6 @@ int lux::build_host_scene(const lux_scene_desc& d, const lux_options& opt, std::
     if (opt.env_importance_sampling && !d.env_data)
         return fail(LUX_ERR_INVALID, "-emis requires an environment map");
     if (d.env_data) {
-        lux_texture_desc et{d.env_width, d.env_height, d.env_format, 0, d.env_data};
-        int rc = make_texture(et, env, opt.texture_storage == LUX_TEXSTORE_HALF ? LUX_TEXSTORE_HALF : LUX_TEXSTORE_FLOAT);
-        if (rc) return rc;
         H.env_w = d.env_width;
         H.env_h = d.env_height;
         H.env_tex = env.obj;

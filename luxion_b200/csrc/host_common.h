@@ -59,14 +59,38 @@ inline void destroy_texture(DevTex& t) {
 // Everything a resident scene needs, built on the host (textures are created on the device
 // here because materials hold their texture objects): per-mesh BLASes concatenated, the
 // TLAS appended after them, instances, materials and the light tables.
+// Allocator whose value-less construct leaves trivially constructible elements uninitialised:
+// the large host arrays of a scene are sized once and first written (and paged in) by the
+// threads that fill them, not zero-filled by one thread beforehand.
+template <class T>
+struct NoInitAlloc : std::allocator<T> {
+    template <class U>
+    struct rebind {
+        using other = NoInitAlloc<U>;
+    };
+    NoInitAlloc() = default;
+    template <class U>
+    NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
+    template <class U>
+    void construct(U* p) noexcept {
+        ::new (static_cast<void*>(p)) U;
+    }
+    template <class U, class... A>
+    void construct(U* p, A&&... a) {
+        ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+    }
+};
+template <class T>
+using HostVec = std::vector<T, NoInitAlloc<T>>;
+
 struct HostScene {
-    std::vector<BVH8Node> nodes;
+    HostVec<BVH8Node> nodes;
     uint32_t tlas_root = 0;           // first TLAS node; nodes from here on are the TLAS
-    std::vector<float4> prims;
+    HostVec<float4> prims;
     std::vector<DevInstance> insts;
     std::vector<uint32_t> tlas_prims;
-    std::vector<float> pos, nrm, uv;
-    std::vector<uint32_t> idx;
+    HostVec<float> pos, nrm, uv;
+    HostVec<uint32_t> idx;
     bool any_n = false, any_uv = false;
     std::vector<DevMaterial> mats;
     std::vector<int> emissive;        // emissive instances
