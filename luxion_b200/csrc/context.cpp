@@ -29,6 +29,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <string>
 #include <thread>
@@ -142,7 +143,38 @@ float half_bits_to_float(uint16_t h) {
 // device, texconv.cu),
 // LUX_TEXSTORE_HALF converts them to binary16, LUX_TEXSTORE_UNORM8 keeps 8-bit texels (16-bit
 // ones become float4). Binary16 texels stay binary16 under every storage.
-int make_texture(const lux_texture_desc& t, DevTex& out, int storage) {
+// Device staging for texel conversion, reused across the textures of one scene build.
+struct TexStage {
+    void* src = nullptr;
+    void* dst = nullptr;
+    size_t src_bytes = 0, dst_bytes = 0;
+    TexStage() = default;
+    TexStage(const TexStage&) = delete;
+    TexStage& operator=(const TexStage&) = delete;
+    ~TexStage() {
+        if (src) cudaFree(src);
+        if (dst) cudaFree(dst);
+    }
+    int reserve(size_t sb, size_t db) {
+        if (sb > src_bytes) {
+            if (src) cudaFree(src);
+            src = nullptr;
+            src_bytes = 0;
+            LUX_CUDA(cudaMalloc(&src, sb));
+            src_bytes = sb;
+        }
+        if (db > dst_bytes) {
+            if (dst) cudaFree(dst);
+            dst = nullptr;
+            dst_bytes = 0;
+            LUX_CUDA(cudaMalloc(&dst, db));
+            dst_bytes = db;
+        }
+        return LUX_OK;
+    }
+};
+
+int make_texture(const lux_texture_desc& t, DevTex& out, int storage, TexStage& stage) {
     if (t.width <= 0 || t.height <= 0 || !t.data) return fail(LUX_ERR_INVALID, "empty texture");
     const size_t n = size_t(t.width) * t.height * 4;
     const void* src = t.data;
@@ -151,20 +183,13 @@ int make_texture(const lux_texture_desc& t, DevTex& out, int storage) {
     const bool to_half = storage == LUX_TEXSTORE_HALF && t.format != LUX_TEX_RGBA16F;
     const bool to_float = (storage == LUX_TEXSTORE_FLOAT && t.format == LUX_TEX_RGBA8) ||
                           (storage != LUX_TEXSTORE_HALF && t.format == LUX_TEX_RGBA16);
-    struct DevBuf {
-        void* p = nullptr;
-        ~DevBuf() {
-            if (p) cudaFree(p);
-        }
-    } dsrc, ddst;
     const void* dev_src = nullptr;
     if (to_half || to_float) {
         const size_t in_bytes = t.format == LUX_TEX_RGBA8 ? 1 : (t.format == LUX_TEX_RGBA32F ? 4 : 2);
-        LUX_CUDA(cudaMalloc(&dsrc.p, n * in_bytes));
-        LUX_CUDA(cudaMalloc(&ddst.p, n * (to_half ? 2 : 4)));
-        LUX_CUDA(cudaMemcpy(dsrc.p, t.data, n * in_bytes, cudaMemcpyHostToDevice));
-        LUX_CUDA(launch_convert_texels(dsrc.p, t.format, to_half ? 1 : 0, ddst.p, n, 0));
-        dev_src = ddst.p;
+        if (int rc = stage.reserve(n * in_bytes, n * (to_half ? 2 : 4))) return rc;
+        LUX_CUDA(cudaMemcpy(stage.src, t.data, n * in_bytes, cudaMemcpyHostToDevice));
+        LUX_CUDA(launch_convert_texels(stage.src, t.format, to_half ? 1 : 0, stage.dst, n, 0));
+        dev_src = stage.dst;
         fmt = to_half ? LUX_TEX_RGBA16F : LUX_TEX_RGBA32F;
     }
     cudaChannelFormatDesc fd;
@@ -344,7 +369,7 @@ bool light_tables(const lux_scene_desc& d, const float* env, std::vector<int>& e
 }  // namespace
 
 int lux::build_host_scene(const lux_scene_desc& d, const lux_options& opt, std::vector<DevTex>& texs,
-                          DevTex& env, HostScene& H) {
+                          DevTex& env, HostScene& H, const std::function<int()>& device_work) {
     const int NM = d.num_meshes;
     const int NI = d.num_instances;
     // ---- textures and the environment map, on their own thread during the BLAS builds ----
@@ -360,12 +385,17 @@ int lux::build_host_scene(const lux_scene_desc& d, const lux_options& opt, std::
             tex_err = g_err;
             return;
         }
-        for (int t = 0; t < d.num_textures && tex_rc == LUX_OK; ++t)
-            tex_rc = make_texture(d.textures[t], texs[tex0 + t], opt.texture_storage);
-        if (tex_rc == LUX_OK && d.env_data) {
-            lux_texture_desc et{d.env_width, d.env_height, d.env_format, 0, d.env_data};
-            tex_rc = make_texture(et, env, opt.texture_storage == LUX_TEXSTORE_HALF ? LUX_TEXSTORE_HALF : LUX_TEXSTORE_FLOAT);
+        {
+            TexStage stage;
+            for (int t = 0; t < d.num_textures && tex_rc == LUX_OK; ++t)
+                tex_rc = make_texture(d.textures[t], texs[tex0 + t], opt.texture_storage, stage);
+            if (tex_rc == LUX_OK && d.env_data) {
+                lux_texture_desc et{d.env_width, d.env_height, d.env_format, 0, d.env_data};
+                tex_rc = make_texture(et, env, opt.texture_storage == LUX_TEXSTORE_HALF ? LUX_TEXSTORE_HALF : LUX_TEXSTORE_FLOAT,
+                                      stage);
+            }
         }
+        if (tex_rc == LUX_OK && device_work) tex_rc = device_work();
         if (tex_rc) tex_err = g_err;
     });
     struct Joiner {
@@ -664,9 +694,10 @@ int lux::build_host_scene(const lux_scene_desc& d, const lux_options& opt, std::
 
 namespace {
 
-int build_scene(lux_ctx* C, const lux_scene_desc& d) {
+// Host build and upload of the scene; device_work runs on the build's device thread.
+int build_scene(lux_ctx* C, const lux_scene_desc& d, const std::function<int()>& device_work) {
     HostScene H;
-    int rc = build_host_scene(d, C->opt, C->texs, C->env, H);
+    int rc = build_host_scene(d, C->opt, C->texs, C->env, H, device_work);
     if (rc) return rc;
     C->instanced_tris = H.instanced_tris;
     C->h_emissive_prefix = H.emissive_prefix;
@@ -677,25 +708,47 @@ int build_scene(lux_ctx* C, const lux_scene_desc& d) {
     return upload_scene(C, H, C->S);
 }
 
+// The wave's arrays are carved from one allocation (each 256-byte aligned), so that a
+// context costs one cudaMalloc and one cudaFree for its whole path state.
 int alloc_wave(lux_ctx* C, int max_paths) {
     DevWave& W = C->W;
     std::memset(&W, 0, sizeof(W));
-    size_t n = size_t(max_paths);
-    int rc;
-    if ((rc = C->alloc(&W.s0, n)) || (rc = C->alloc(&W.s1, n)) || (rc = C->alloc(&W.s2, n)) ||
-        (rc = C->alloc(&W.s3, n)) || (rc = C->alloc(&W.s4, n)) || (rc = C->alloc(&W.queue[0], n)) ||
-        (rc = C->alloc(&W.queue[1], n)) || (rc = C->alloc(&W.hit, n)) || (rc = C->alloc(&W.hit_prim, n)) ||
-        (rc = C->alloc(&W.sh_o, n)) || (rc = C->alloc(&W.sh_d, n)) || (rc = C->alloc(&W.sh_queue, n)) ||
-        (rc = C->alloc(&W.sh_hit, n)) || (rc = C->alloc(&W.sh_prim, n)) || (rc = C->alloc(&W.ctr, 1)) ||
-        (rc = C->alloc(&W.wave_iter, 4)))
-        return rc;
+    const size_t n = size_t(max_paths);
+    size_t off = 0;
+    std::vector<std::pair<void**, size_t>> parts;
+    auto take = [&](auto*& p, size_t count) {
+        off = (off + 255) & ~size_t(255);
+        parts.emplace_back(reinterpret_cast<void**>(&p), off);
+        off += count * sizeof(*p);
+    };
+    take(W.s0, n);
+    take(W.s1, n);
+    take(W.s2, n);
+    take(W.s3, n);
+    take(W.s4, n);
+    take(W.queue[0], n);
+    take(W.queue[1], n);
+    take(W.hit, n);
+    take(W.hit_prim, n);
+    take(W.sh_o, n);
+    take(W.sh_d, n);
+    take(W.sh_queue, n);
+    take(W.sh_hit, n);
+    take(W.sh_prim, n);
+    take(W.ctr, 1);
+    take(W.wave_iter, 4);
+    char* sort_temp = nullptr;
     if (C->opt.ray_sorting) {
-        if ((rc = C->alloc(&W.keys, n)) || (rc = C->alloc(&W.keys_alt, n)) || (rc = C->alloc(&W.queue_alt, n))) return rc;
+        take(W.keys, n);
+        take(W.keys_alt, n);
+        take(W.queue_alt, n);
         C->sort_temp_bytes = morton_sort_temp_bytes(max_paths);
-        char* t = nullptr;
-        if ((rc = C->alloc(&t, C->sort_temp_bytes))) return rc;
-        C->sort_temp = t;
+        take(sort_temp, C->sort_temp_bytes);
     }
+    char* base = nullptr;
+    if (int rc = C->alloc(&base, off)) return rc;
+    for (auto& pt : parts) *pt.first = base + pt.second;
+    if (C->opt.ray_sorting) C->sort_temp = sort_temp;
     W.npix = C->npix;
     W.width = C->width;
     W.height = C->height;
@@ -944,19 +997,24 @@ int lux_init(const lux_scene_desc* scene, const lux_options* opt, lux_ctx** out)
             return bail(fail(LUX_ERR_CUDA, "cudaStreamCreate failed"));
         C->own_stream = true;
     }
-    int rc = build_scene(C, d);
-    if (rc) return bail(rc);
     // samples kept in flight together: about 8M paths, at least one sample
     int spw = o.spp_per_wave > 0 ? o.spp_per_wave : std::max(1, (8 << 20) / C->npix);
     spw = std::max(1, std::min(spw, 1 << 16));
     C->spp_per_wave = spw;
-    if ((rc = alloc_wave(C, spw * C->npix))) return bail(rc);
-    if ((rc = C->alloc(&C->image, size_t(C->npix) * 3))) return bail(rc);
-    if (o.precision == LUX_PRECISION_COMPENSATED && (rc = C->alloc(&C->comp, size_t(C->npix) * 3))) return bail(rc);
-    if ((rc = C->alloc(&C->rgba, size_t(C->npix) * 4))) return bail(rc);
-    if (cudaMemset(C->image, 0, size_t(C->npix) * 3 * sizeof(float)) != cudaSuccess)
-        return bail(fail(LUX_ERR_CUDA, "memset"));
-    if (C->comp) cudaMemset(C->comp, 0, size_t(C->npix) * 3 * sizeof(float));
+    // The wave buffers and the image do not depend on the scene: the scene build's device
+    // thread allocates them after the textures, while this thread builds the BVHs.
+    int rc = build_scene(C, d, [&]() {
+        int r = alloc_wave(C, spw * C->npix);
+        if (!r) r = C->alloc(&C->image, size_t(C->npix) * 3);
+        if (!r && o.precision == LUX_PRECISION_COMPENSATED) r = C->alloc(&C->comp, size_t(C->npix) * 3);
+        if (!r) r = C->alloc(&C->rgba, size_t(C->npix) * 4);
+        if (!r && cudaMemset(C->image, 0, size_t(C->npix) * 3 * sizeof(float)) != cudaSuccess)
+            r = fail(LUX_ERR_CUDA, "memset");
+        if (!r && C->comp && cudaMemset(C->comp, 0, size_t(C->npix) * 3 * sizeof(float)) != cudaSuccess)
+            r = fail(LUX_ERR_CUDA, "memset");
+        return r;
+    });
+    if (rc) return bail(rc);
     cudaEventCreate(&C->ev[0]);
     cudaEventCreate(&C->ev[1]);
     // occupancy queries happen here, never inside a stream capture

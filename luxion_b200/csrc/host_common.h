@@ -11,6 +11,7 @@
 
 #include <cstdint>
 #include <cstring>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -109,9 +110,11 @@ int validate_scene_desc(const lux_scene_desc& d);
 
 // Build of one validated scene description with the given options (texture storage,
 // precision, which light tables -dmis / -emis require). Textures are appended to texs; the
-// environment map goes to env.
+// environment map goes to env. Textures are created on a second thread while the BVHs are
+// built; device_work, when given, runs on that thread after them and its status is returned
+// like a texture failure. The thread is joined before the function returns.
 int build_host_scene(const lux_scene_desc& d, const lux_options& opt, std::vector<DevTex>& texs, DevTex& env,
-                     HostScene& H);
+                     HostScene& H, const std::function<int()>& device_work = nullptr);
 
 // Upload the light tables of a host scene and set its environment and Morton box fields.
 // Owner provides up(T** dst, const T* src, size_t n), which records the allocation.
