@@ -223,16 +223,17 @@ void build_binary(const float* boxes, int n, Binary& B) {
 }
 
 // Quantise the child boxes of one 8-wide node. The node box is first widened by a relative
-// 1e-5 of its largest extent (plus 1e-7 of its coordinate magnitude) and every child plane
-// is rounded outward by a further 1% of a quantisation step, which dominates the rounding
-// error of the device slab test (a few ulps of the node extent).
+// 1e-4 of its largest extent (plus 1e-7 of its coordinate magnitude), at least 1.27 % of a
+// quantisation step on every axis, and every child plane is rounded outward by a further 1 %
+// of a step. Either margin dominates the rounding error of the device slab test: at most
+// 2^-9 of a step beyond a relative 2^-19 of the plane distance, which the device widens.
 void encode_node(BVH8Node& N, const Box& nb, const Box* cbox, const bool* used) {
     double mext = 0.0, mabs = 0.0;
     for (int a = 0; a < 3; ++a) {
         mext = std::max(mext, double(nb.hi[a]) - double(nb.lo[a]));
         mabs = std::max(mabs, std::max(std::fabs(double(nb.lo[a])), std::fabs(double(nb.hi[a]))));
     }
-    const double pad = 1e-5 * mext + 1e-7 * mabs + 1e-30;
+    const double pad = 1e-4 * mext + 1e-7 * mabs + 1e-30;
     double hi_d[3];
     for (int a = 0; a < 3; ++a) {
         double lo_d = double(nb.lo[a]) - pad;

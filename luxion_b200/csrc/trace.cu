@@ -64,8 +64,9 @@ LUX_DI TRay make_ray(f3 o, f3 d) {
     return r;
 }
 
-// byte s of w as a float: one byte permute builds 0x4B0000bb (2^23 + byte), one add removes 2^23
-LUX_DI float ubyte(uint32_t w, int s) { return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u | uint32_t(s))) - 8388608.0f; }
+// Byte s of w as the float 2^23 + 256 * byte: one byte permute builds 0x4B00bb00. The 2^23
+// bias is folded into the per-node plane constant (visit_node), so no add removes it.
+LUX_DI float ubyte_biased(uint32_t w, int s) { return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7504u | (uint32_t(s) << 4))); }
 
 // Intersect the 8 child boxes of node ni. Returns internal-child hits as a key mask
 // (bit (slot ^ oct)), the leaf primitive mask (bit offset), child_base and tri_base.
@@ -80,8 +81,15 @@ LUX_DI void visit_node(const uint4* __restrict__ nodes, uint32_t ni, const TRay&
     imask = w0.w >> 24;
     child_base = w1.x;
     tri_base = w1.y;
-    float ax = sx * r.idir.x, ay = sy * r.idir.y, az = sz * r.idir.z;
+    // plane q of an axis lies at t = q * a + b with a = scale * idir, b = (p - o) * idir.
+    // It is evaluated as fma(2^23 + 256 q, a / 256, b - 2^15 a): a / 256 is exact, and the
+    // rounding of the folded constant adds at most 2^-9 of a quantisation step (the host pads
+    // every plane by at least 1 % of a step).
+    float ax = sx * r.idir.x * 0.00390625f, ay = sy * r.idir.y * 0.00390625f, az = sz * r.idir.z * 0.00390625f;
     float bx = (px - r.o.x) * r.idir.x, by = (py - r.o.y) * r.idir.y, bz = (pz - r.o.z) * r.idir.z;
+    bx = fmaf(-8388608.0f, ax, bx);
+    by = fmaf(-8388608.0f, ay, by);
+    bz = fmaf(-8388608.0f, az, bz);
     // near/far quantised planes per axis, by ray octant
     const bool fx = r.oct & 1, fy = r.oct & 2, fz = r.oct & 4;
     uint32_t nx0 = fx ? w3.z : w2.x, nx1 = fx ? w3.w : w2.y, fx0 = fx ? w2.x : w3.z, fx1 = fx ? w2.y : w3.w;
@@ -94,8 +102,10 @@ LUX_DI void visit_node(const uint4* __restrict__ nodes, uint32_t ni, const TRay&
         const int b = s & 3;
         uint32_t wnx = s < 4 ? nx0 : nx1, wny = s < 4 ? ny0 : ny1, wnz = s < 4 ? nz0 : nz1;
         uint32_t wfx = s < 4 ? fx0 : fx1, wfy = s < 4 ? fy0 : fy1, wfz = s < 4 ? fz0 : fz1;
-        float tnx = fmaf(ubyte(wnx, b), ax, bx), tny = fmaf(ubyte(wny, b), ay, by), tnz = fmaf(ubyte(wnz, b), az, bz);
-        float tfx = fmaf(ubyte(wfx, b), ax, bx), tfy = fmaf(ubyte(wfy, b), ay, by), tfz = fmaf(ubyte(wfz, b), az, bz);
+        float tnx = fmaf(ubyte_biased(wnx, b), ax, bx), tny = fmaf(ubyte_biased(wny, b), ay, by),
+              tnz = fmaf(ubyte_biased(wnz, b), az, bz);
+        float tfx = fmaf(ubyte_biased(wfx, b), ax, bx), tfy = fmaf(ubyte_biased(wfy, b), ay, by),
+              tfz = fmaf(ubyte_biased(wfz, b), az, bz);
         float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
         float tf = fminf(fminf(tfx, tfy), fminf(tfz, tmax));
         uint32_t meta = ((s < 4 ? w1.z : w1.w) >> (8 * b)) & 0xffu;
