@@ -148,6 +148,18 @@ enum { LUX_PRECISION_PLAIN = 0, LUX_PRECISION_COMPENSATED = 1 };
  * keeps 8-bit texels as they are (4 B/texel, filtered by the hardware unorm path); HALF
  * stores IEEE binary16 (the precision form). */
 enum { LUX_TEXSTORE_FLOAT = 0, LUX_TEXSTORE_UNORM8 = 1, LUX_TEXSTORE_HALF = 2 };
+/* Material debug views (PathTracerOptions::material_debug_mode, include/pathtrace/
+ * pathtracer_options.h:5; render_material_debug_mode, src/material_debug_render.cu:3-26):
+ * trace depth 1, a camera hit shows one material channel, the display skips tone mapping. */
+enum {
+    LUX_MATDEBUG_OFF = 0,
+    LUX_MATDEBUG_ALBEDO = 1,
+    LUX_MATDEBUG_NORMAL = 2,     /* shading normal * 0.5 + 0.5                          */
+    LUX_MATDEBUG_NORMAL_MAP = 3, /* raw normal-map texel, (0.5, 0.5, 1) without one      */
+    LUX_MATDEBUG_ROUGHNESS = 4,
+    LUX_MATDEBUG_METALLIC = 5,
+    LUX_MATDEBUG_ALPHA = 6
+};
 
 typedef struct lux_options {
     int32_t direct_light_sampling;       /* -dmis                                            */
@@ -162,6 +174,11 @@ typedef struct lux_options {
     int32_t texture_storage;             /* LUX_TEXSTORE_*                                    */
     int32_t device;                      /* CUDA device ordinal                              */
     void* stream;                        /* cudaStream_t to launch on; NULL = a private one  */
+    int32_t material_debug_mode;         /* LUX_MATDEBUG_*                                   */
+    int32_t debug_bvh;                   /* 1: BVH heatmap of camera rays (PathTracerOptions::
+                                          * debug_bvh, src/kernels/draw_bvh.cu:6-35): each
+                                          * sample adds (BVH8 node visits + triangle tests)
+                                          * * 0.001 to every channel of its pixel             */
 } lux_options;
 
 typedef struct lux_ctx lux_ctx;

@@ -415,7 +415,9 @@ class PathTracerOptions:
     def to_options(self, **kw) -> Options:
         return default_options(direct_light_sampling=int(self.direct_light_sampling),
                                env_importance_sampling=int(self.environment_map_importance_sampling),
-                               color_mode=int(self.color_mode), envmap_intensity=float(self.envmap_intensity), **kw)
+                               color_mode=int(self.color_mode), envmap_intensity=float(self.envmap_intensity),
+                               material_debug_mode=int(self.material_debug_mode), debug_bvh=int(bool(self.debug_bvh)),
+                               **kw)
 
 
 _state: Optional[Renderer] = None

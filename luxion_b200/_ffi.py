@@ -28,6 +28,8 @@ ALPHA_OPAQUE, ALPHA_MASK, ALPHA_BLEND = 0, 1, 2
 TONEMAP_REINHARD, TONEMAP_AGX, TONEMAP_ACES = 0, 1, 2
 PRECISION_PLAIN, PRECISION_COMPENSATED = 0, 1
 TEXSTORE_FLOAT, TEXSTORE_UNORM8, TEXSTORE_HALF = 0, 1, 2
+(MATDEBUG_OFF, MATDEBUG_ALBEDO, MATDEBUG_NORMAL, MATDEBUG_NORMAL_MAP, MATDEBUG_ROUGHNESS, MATDEBUG_METALLIC,
+ MATDEBUG_ALPHA) = range(7)
 TRACE_STATIC_MAX_RAYS = 65536  # LUX_TRACE_STATIC_MAX_RAYS
 
 # path-state layout (LUX_PS_*)
@@ -88,7 +90,7 @@ class Options(C.Structure):
                 ("trace_depth", C.c_int32), ("ray_sorting", C.c_int32),
                 ("precision", C.c_int32), ("spp_per_wave", C.c_int32),
                 ("use_graph", C.c_int32), ("texture_storage", C.c_int32), ("device", C.c_int32),
-                ("stream", C.c_void_p)]
+                ("stream", C.c_void_p), ("material_debug_mode", C.c_int32), ("debug_bvh", C.c_int32)]
 
 
 class Stats(C.Structure):
@@ -148,6 +150,8 @@ def default_options(**kw) -> Options:
     o.texture_storage = TEXSTORE_FLOAT
     o.device = 0
     o.stream = None
+    o.material_debug_mode = MATDEBUG_OFF
+    o.debug_bvh = 0
     for k, v in kw.items():
         setattr(o, k, v)
     return o

@@ -1,16 +1,21 @@
 """Headless command line of the renderer, with the reference's flags (src/main.cpp:81-147):
 
     python -m luxion_b200 SCENE [-e|--envmap ENVMAP] [-i|--iterations N] [-o|--output NAME]
-                                [-dmis] [-emis] [-lock]
+                                [-dmis] [-emis] [-lock] [-debug-material N] [-debug-bvh]
 
 SCENE is a glTF 2.0 file (.glb or .gltf, loaded as the reference's loader does: luxion_b200.gltf)
 or a procedural scene: cornell (the 36-triangle Cornell box), random[:SEED[:TRIS]] (the
 instanced test scene) or furnace. ENVMAP is an OpenEXR (.exr) or Radiance (.hdr) image, or a
 float32 .npy array of HxWx3 or HxWx4 texels, replacing the scene's environment map. -lock is
 accepted and ignored (it locks the interactive camera).
+-debug-material N (1 albedo, 2 world normal, 3 normal map, 4 roughness, 5 metallic, 6 alpha) and
+-debug-bvh select the debug views the reference offers in its ImGui panel
+(src/app/render_imgui.cpp:336-345): PathTracerOptions::material_debug_mode and debug_bvh.
 The image is written as NAME.png the way the reference's saveImage does
 (src/app/save_image.cpp:42-84): the accumulated sum divided by the sample count, ACES, gamma
-0.45, x mirrored, each channel clamped to [0, 1] and truncated from value * 255.
+0.45, x mirrored, each channel clamped to [0, 1] and truncated from value * 255. A material
+debug view is written as the reference displays it (src/kernels/image_kernels.cu:20-33): the
+mean without tone map or gamma, x mirrored like every saved image.
 """
 from __future__ import annotations
 
@@ -24,13 +29,15 @@ from typing import List, Optional
 import numpy as np
 
 USAGE = ("Usage: %s SCENEFILE [-e|--envmap ENVMAP] [-i|--iterations N] [-o|--output NAME] [-dmis] [-emis] [-lock]\n"
-         "  SCENEFILE: a .glb/.gltf file, or cornell | random[:SEED[:TRIS]] | furnace")
+         "       [-debug-material N] [-debug-bvh]\n"
+         "  SCENEFILE: a .glb/.gltf file, or cornell | random[:SEED[:TRIS]] | furnace\n"
+         "  -debug-material N: 1 albedo, 2 world normal, 3 normal map, 4 roughness, 5 metallic, 6 alpha")
 
 
 def parse_args(argv: List[str]) -> dict:
     """Parse the reference's flags; raise ValueError with its messages on bad input."""
     out = {"scene": None, "envmap": None, "iterations": 5000, "output": None, "dmis": False, "emis": False,
-           "lock": False}
+           "lock": False, "debug_material": 0, "debug_bvh": False}
     i = 0
     while i < len(argv):
         a = argv[i]
@@ -58,6 +65,16 @@ def parse_args(argv: List[str]) -> dict:
             out["emis"] = True
         elif a == "-lock":
             out["lock"] = True
+        elif a == "-debug-material":
+            if i + 1 >= len(argv):
+                raise ValueError(f"Error: {a} requires a number")
+            v = argv[i + 1]
+            if v not in ("1", "2", "3", "4", "5", "6"):
+                raise ValueError(f"Error: invalid material debug mode '{v}' (1..6)")
+            out["debug_material"] = int(v)
+            i += 1
+        elif a == "-debug-bvh":
+            out["debug_bvh"] = True
         elif out["scene"] is None:
             out["scene"] = a
         else:
@@ -65,6 +82,8 @@ def parse_args(argv: List[str]) -> dict:
         i += 1
     if out["scene"] is None:
         raise ValueError("usage")
+    if out["debug_material"] and out["debug_bvh"]:
+        raise ValueError("Error: -debug-material and -debug-bvh are exclusive")
     return out
 
 
@@ -74,10 +93,12 @@ def aces(x: np.ndarray) -> np.ndarray:
     return np.clip((x * (a * x + b)) / (x * (c * x + d) + e), np.float32(0), np.float32(1))
 
 
-def to_png_bytes(image_sum: np.ndarray, samples: int) -> np.ndarray:
-    """HxWx3 uint8 of saveImage: mean, ACES, gamma 0.45, x mirrored, clamp * 255 truncated."""
+def to_png_bytes(image_sum: np.ndarray, samples: int, tonemap: bool = True) -> np.ndarray:
+    """HxWx3 uint8 of saveImage: mean, ACES, gamma 0.45, x mirrored, clamp * 255 truncated.
+    tonemap=False leaves out ACES and gamma (a material debug view)."""
     pix = image_sum.astype(np.float32) / np.float32(samples)
-    pix = np.power(aces(pix), np.float32(0.45))
+    if tonemap:
+        pix = np.power(aces(pix), np.float32(0.45))
     pix = pix[:, ::-1, :]
     return (np.clip(pix, np.float32(0), np.float32(1)) * np.float32(255)).astype(np.uint8)
 
@@ -186,7 +207,8 @@ def main(argv: Optional[List[str]] = None) -> int:
         d = scene.desc
         d.env_width, d.env_height, d.env_format = env.shape[1], env.shape[0], _ffi.TEX_RGBA32F
         d.env_data = keep.ctypes.data
-    opt = lx.default_options(direct_light_sampling=int(a["dmis"]), env_importance_sampling=int(a["emis"]))
+    opt = lx.default_options(direct_light_sampling=int(a["dmis"]), env_importance_sampling=int(a["emis"]),
+                             material_debug_mode=a["debug_material"], debug_bvh=int(a["debug_bvh"]))
     try:
         r = lx.Renderer(scene, opt)
     except lx.LuxError as e:
@@ -202,7 +224,7 @@ def main(argv: Optional[List[str]] = None) -> int:
     out = name + ".png"
     if os.path.dirname(out):
         os.makedirs(os.path.dirname(out), exist_ok=True)
-    write_png(out, to_png_bytes(img, a["iterations"]))
+    write_png(out, to_png_bytes(img, a["iterations"], tonemap=not a["debug_material"]))
     rays = st["rays_radiance"] + st["rays_shadow"]
     print(f"Saved {out}. {a['iterations']} samples of {img.shape[1]}x{img.shape[0]} in {dt:.3f} s, "
           f"{rays / dt / 1e6:.1f} Mrays/s")

@@ -775,6 +775,13 @@ int enqueue_wave(lux_ctx* C, int ns, const cudaEvent_t* ev) {
     for (int b = 0; b < depth; ++b) {
         if (C->opt.ray_sorting) LUX_CUDA(launch_morton_sort(C->S, W, b, C->sort_temp, C->sort_temp_bytes, st));
         rec();
+        if (C->opt.debug_bvh) {
+            // BVH heatmap: the counting traversal writes the camera ray's colour; no shading
+            LUX_CUDA(launch_trace(C->S, W, b, 3, 0, st));
+            rec();
+            rec();
+            continue;
+        }
         LUX_CUDA(launch_trace(C->S, W, b, 0, nee, st));
         if (nee) LUX_CUDA(launch_trace(C->S, W, b, nee == 2 ? 2 : 1, 0, st));
         rec();
@@ -954,6 +961,14 @@ int lux_init(const lux_scene_desc* scene, const lux_options* opt, lux_ctx** out)
         return fail(LUX_ERR_INVALID, "unknown texture storage");
     int tdepth = o.trace_depth > 0 ? o.trace_depth : d.trace_depth;
     if (tdepth <= 0 || tdepth > kMaxDepth) return fail(LUX_ERR_INVALID, "trace depth must be in 1..64");
+    if (o.material_debug_mode < LUX_MATDEBUG_OFF || o.material_debug_mode > LUX_MATDEBUG_ALPHA)
+        return fail(LUX_ERR_INVALID, "material_debug_mode must be in 0..6");
+    if (o.debug_bvh != 0 && o.debug_bvh != 1) return fail(LUX_ERR_INVALID, "debug_bvh must be 0 or 1");
+    if (o.debug_bvh && o.material_debug_mode)
+        return fail(LUX_ERR_UNSUPPORTED, "the BVH heatmap and a material debug view are exclusive");
+    // debug views trace camera rays only (src/pathtrace.cu:107 forces trace depth 1 for the
+    // material views); their camera rays are seeded with that depth as well
+    if (o.material_debug_mode || o.debug_bvh) tdepth = 1;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(LUX_ERR_NO_DEVICE, "no CUDA device");
     if (o.device < 0 || o.device >= ndev) return fail(LUX_ERR_INVALID, "device ordinal out of range");
@@ -970,6 +985,7 @@ int lux_init(const lux_scene_desc* scene, const lux_options* opt, lux_ctx** out)
     C->dopt.trace_depth = tdepth;
     C->dopt.color_mode = o.color_mode;
     C->dopt.precision = o.precision;
+    C->dopt.material_debug = o.material_debug_mode;
     C->width = d.camera.width;
     C->height = d.camera.height;
     C->npix = C->width * C->height;
@@ -1018,7 +1034,7 @@ int lux_init(const lux_scene_desc* scene, const lux_options* opt, lux_ctx** out)
     cudaEventCreate(&C->ev[0]);
     cudaEventCreate(&C->ev[1]);
     // occupancy queries happen here, never inside a stream capture
-    for (int m = 0; m < 3; ++m) trace_grid_blocks(m);
+    for (int m = 0; m < 4; ++m) trace_grid_blocks(m);
     shade_grid_blocks();
     if (cudaDeviceSynchronize() != cudaSuccess) return bail(fail(LUX_ERR_CUDA, cudaGetErrorString(cudaGetLastError())));
     *out = C;
@@ -1042,7 +1058,7 @@ int lux_render_iter(lux_ctx* C, int iter, uint8_t* rgba8_dev) {
     C->spp_per_wave = save;
     if (rc) return rc;
     if (rgba8_dev) {
-        LUX_CUDA(launch_tonemap(C->image, rgba8_dev, C->npix, float(iter), C->opt.color_mode, C->stream));
+        LUX_CUDA(launch_tonemap(C->image, rgba8_dev, C->npix, float(iter), C->opt.material_debug_mode ? -1 : C->opt.color_mode, C->stream));
         LUX_CUDA(cudaStreamSynchronize(C->stream));
     }
     return LUX_OK;
@@ -1068,7 +1084,7 @@ int lux_copy_rgba8(lux_ctx* C, uint8_t* rgba_host) {
     if (!C || !rgba_host) return fail(LUX_ERR_INVALID, "NULL argument");
     cudaSetDevice(C->device);
     float it = float(std::max(1, C->accumulated));
-    LUX_CUDA(launch_tonemap(C->image, C->rgba, C->npix, it, C->opt.color_mode, C->stream));
+    LUX_CUDA(launch_tonemap(C->image, C->rgba, C->npix, it, C->opt.material_debug_mode ? -1 : C->opt.color_mode, C->stream));
     LUX_CUDA(cudaMemcpyAsync(rgba_host, C->rgba, size_t(C->npix) * 4, cudaMemcpyDeviceToHost, C->stream));
     LUX_CUDA(cudaStreamSynchronize(C->stream));
     return LUX_OK;

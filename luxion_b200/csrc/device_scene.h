@@ -106,6 +106,7 @@ struct DevOptions {
     int trace_depth;
     int color_mode;
     int precision;
+    int material_debug;  // LUX_MATDEBUG_* (trace depth is 1 when set)
 };
 
 // Per-bounce device counters, zeroed once per wave (one memset):

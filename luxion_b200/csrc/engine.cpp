@@ -278,6 +278,8 @@ int lux_engine_create(const lux_scene_desc* const* scenes, int num_scenes, const
     else lux_default_options(&o);
     if (o.texture_storage < LUX_TEXSTORE_FLOAT || o.texture_storage > LUX_TEXSTORE_HALF)
         return fail(LUX_ERR_INVALID, "unknown texture storage");
+    if (o.material_debug_mode || o.debug_bvh)
+        return fail(LUX_ERR_UNSUPPORTED, "debug views are rendered by lux_init contexts, not by the engine");
     lux_engine_config c{};
     if (cfg) c = *cfg;
     if (c.max_paths < 0 || c.max_jobs < 0 || c.trace_blocks < 0 || c.hbm_budget_bytes < 0)

@@ -183,6 +183,38 @@ LUX_DI f3 get_emission(const DevMaterial& m, float u, float v) {
     return e;
 }
 
+// The normal-map texel get_normal reads (src/material_queries.cu:32-40), or (0.5, 0.5, 1)
+// without a normal texture.
+LUX_DI f3 normal_map_texel(const DevMaterial& m, float u, float v) {
+    if (!(m.flags & kMatNormalTex)) return mk(0.5f, 0.5f, 1.0f);
+    tt_apply(m.normal_tt, u, v);
+    float4 t = tex(m.normal_tex, u, v);
+    return mk(t.x, t.y, t.z);
+}
+// get_alpha (src/material_queries.cu:119-137)
+LUX_DI float get_alpha(const DevMaterial& m, float u, float v) {
+    if (m.alpha_mode == 0) return 1.0f;
+    float alpha = m.alpha;
+    if (m.flags & kMatAlbedoTex) {
+        tt_apply(m.albedo_tt, u, v);
+        alpha *= tex(m.albedo_tex, u, v).w;
+    }
+    if (m.alpha_mode == 1) return alpha >= m.alpha_cutoff ? 1.0f : 0.0f;
+    return alpha;
+}
+// render_material_debug_mode (src/material_debug_render.cu:3-26)
+LUX_DI f3 material_debug_color(int mode, f3 mc, f3 normal, f3 nmap, float rough, float metal, float alpha) {
+    switch (mode) {
+        case 1: return mc;
+        case 2: return normal * 0.5f + mk(0.5f, 0.5f, 0.5f);
+        case 3: return nmap;
+        case 4: return mk(rough, rough, rough);
+        case 5: return mk(metal, metal, metal);
+        case 6: return mk(alpha, alpha, alpha);
+    }
+    return mk(0.0f, 0.0f, 0.0f);
+}
+
 // ---- Cook-Torrance (src/shaders/cook_torrance.cu:8-331)
 LUX_DI float D_GGX(f3 h, f3 n, float alpha) {
     float ndh = dot(n, h);
@@ -423,6 +455,8 @@ struct PathState {
 
 // shadePath for one path; returns true if the path survives (is not killed).
 // sh_t: DL shadow hit t (or env occlusion); sh_* the DL shadow hit record.
+// MATDBG: the instantiation that also renders the material debug views (O.material_debug).
+template <bool MATDBG>
 LUX_DI bool shade_one(const DevScene& S, const DevOptions& O, int depth, PathState& p, float t, int inst, int prim,
                       float bu, float bv, float sh_t, int sh_inst, int sh_prim, float sh_u, float sh_v) {
     Rng rng = Rng::seeded(p.iter, p.pixel, depth);
@@ -435,6 +469,12 @@ LUX_DI bool shade_one(const DevScene& S, const DevOptions& O, int depth, PathSta
         f3 normal = get_normal(m, is);
         float rough, metal;
         get_mr(m, is.u, is.v, rough, metal);
+        if (MATDBG && O.material_debug) {
+            // the debug view replaces the colour and ends the path (shade_path.cu:154-164)
+            p.color = material_debug_color(O.material_debug, mc, normal, normal_map_texel(m, is.u, is.v), rough, metal,
+                                           get_alpha(m, is.u, is.v));
+            return false;
+        }
         f3 emission = get_emission(m, is.u, is.v);
         bool is_spec = rough < kSPEC_ROUGH;
         f3 nf = dot(-p.d, normal) < 0.0f ? -normal : normal;
@@ -594,7 +634,7 @@ __global__ void __launch_bounds__(kShadeBlock, 16) k_camera(DevScene S, DevWave 
 // texture fetches and gathers, and hiding that latency with more warps pays more than the
 // register spills cost (shade per 16-spp step of the 1M-triangle 1080p workload: 28.3 ms at
 // 5 blocks per SM, 22.6 at 8, 20.4 at 12, 18.8 at 16).
-template <bool JOBS>
+template <bool JOBS, bool MATDBG>
 __global__ void __launch_bounds__(kShadeBlock, 16) k_shade(const __grid_constant__ DevScene S0, DevWave W, DevOptions O,
                                                        int bounce, int compact) {
     const int n = *(volatile int*)&W.ctr->count[bounce];
@@ -635,7 +675,7 @@ __global__ void __launch_bounds__(kShadeBlock, 16) k_shade(const __grid_constant
                     spr = W.sh_prim[slot];
                 }
             }
-            alive = shade_one(S, O, depth, p, h.x, inst, prim, h.y, h.z, sh_t, si, spr, su, sv) && job_compact;
+            alive = shade_one<MATDBG>(S, O, depth, p, h.x, inst, prim, h.y, h.z, sh_t, si, spr, su, sv) && job_compact;
             W.s3[pid] = make_float4(p.color.x, p.color.y, p.color.z, __int_as_float(p.iter));
             if (alive) {
                 W.s0[pid] = make_float4(p.o.x, p.o.y, p.o.z, p.last_pdf);
@@ -821,10 +861,12 @@ __global__ void k_tonemap(const float* __restrict__ image, uchar4* __restrict__ 
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += gridDim.x * blockDim.x) {
         float inv = __frcp_rn(iter);
         f3 p = mk(image[i * 3], image[i * 3 + 1], image[i * 3 + 2]) * inv;
-        if (mode == 0) p = mk(p.x / (p.x + 1.0f), p.y / (p.y + 1.0f), p.z / (p.z + 1.0f));
-        else if (mode == 1) p = agx(p);
-        else p = aces(p);
-        p = vpow(p, 0.45f);
+        if (mode >= 0) {  // mode < 0: material debug view, shown without tone map or gamma
+            if (mode == 0) p = mk(p.x / (p.x + 1.0f), p.y / (p.y + 1.0f), p.z / (p.z + 1.0f));
+            else if (mode == 1) p = agx(p);
+            else p = aces(p);
+            p = vpow(p, 0.45f);
+        }
         out[i] = make_uchar4((unsigned char)gclampi(int(double(p.x) * 255.0), 0, 255),
                              (unsigned char)gclampi(int(double(p.y) * 255.0), 0, 255),
                              (unsigned char)gclampi(int(double(p.z) * 255.0), 0, 255), 0);
@@ -856,7 +898,7 @@ __global__ void k_shade_ext(DevScene S, DevOptions O, float* paths, const uint32
             float su = __uint_as_float(h[8]), sv = __uint_as_float(h[9]);
             int si = int(h[6]), spr = int(h[7]);
             if (O.env) si = -1;
-            bool survived = shade_one(S, O, depth, p, t, inst, prim, __uint_as_float(h[3]), __uint_as_float(h[4]),
+            bool survived = shade_one<true>(S, O, depth, p, t, inst, prim, __uint_as_float(h[3]), __uint_as_float(h[4]),
                                       __uint_as_float(h[5]), si, spr, su, sv);
             alive = survived && compact;
             f[0] = p.o.x; f[1] = p.o.y; f[2] = p.o.z;
@@ -910,8 +952,8 @@ int shade_grid_blocks() {
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         int per_jobs = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_shade<false>, kShadeBlock, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_jobs, k_shade<true>, kShadeBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_shade<false, false>, kShadeBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_jobs, k_shade<true, false>, kShadeBlock, 0);
         per = std::min(per, per_jobs);
         cached = sms * (per > 0 ? per : 1);
     }
@@ -928,8 +970,9 @@ cudaError_t launch_camera(const DevScene& S, const DevWave& W, const DevOptions&
 
 cudaError_t launch_shade(const DevScene& S, const DevWave& W, const DevOptions& O, int bounce, int compact,
                          cudaStream_t st) {
-    if (W.path_job) k_shade<true><<<shade_grid_blocks(), kShadeBlock, 0, st>>>(S, W, O, bounce, compact);
-    else k_shade<false><<<shade_grid_blocks(), kShadeBlock, 0, st>>>(S, W, O, bounce, compact);
+    if (W.path_job) k_shade<true, false><<<shade_grid_blocks(), kShadeBlock, 0, st>>>(S, W, O, bounce, compact);
+    else if (O.material_debug) k_shade<false, true><<<shade_grid_blocks(), kShadeBlock, 0, st>>>(S, W, O, bounce, compact);
+    else k_shade<false, false><<<shade_grid_blocks(), kShadeBlock, 0, st>>>(S, W, O, bounce, compact);
     return cudaGetLastError();
 }
 

@@ -213,6 +213,7 @@ struct Lane {
     int inst_flags;
     uint32_t inst_prim_base;
     int pixel, iter;    // alpha-blend hash key
+    int work;           // BVH heatmap (mode 3): node visits + triangle tests
     bool done;
 };
 
@@ -252,6 +253,7 @@ struct Tracer {
         L.inst_flags = 0;
         L.inst_prim_base = 0;
         L.done = false;
+        L.work = 0;
         // root group: a single internal child (slot 0) = the TLAS root, at key oct
         L.g = make_uint2(root, (1u << 8) | (1u << L.cur.oct));
         L.t = make_uint2(0u, 0u);
@@ -270,6 +272,7 @@ struct Tracer {
         if (keys) push(L, make_uint2(L.g.x, (imask << 8) | keys));
         uint32_t nkeys, nimask, cbase, tbase, tmask;
         visit_node(S.nodes, child, L.cur, limit(L), nkeys, nimask, cbase, tbase, tmask);
+        if (MODE == 3) ++L.work;
         L.g = make_uint2(cbase, (nimask << 8) | nkeys);
         if (tmask) {
             if (L.inst >= 0) L.t = make_uint2(L.inst_prim_base + tbase, kTagTri | tmask);
@@ -285,6 +288,7 @@ struct Tracer {
         L.t.y = m ? (kTagTri | m) : 0u;
         float t, u, v;
         int prim;
+        if (MODE == 3) ++L.work;
         if (!mt_test(S.prims, L.t.x + uint32_t(k), L.cur, t, u, v, prim)) return;
         if (!(t <= L.tmax)) return;
         if (MODE != 2 && !better(t, L.inst, prim, L.best)) return;
@@ -347,7 +351,7 @@ struct TraceArgs {
     DevScene S;
     DevWave W;
     int bounce;
-    int mode;    // 0 radiance, 1 DL shadow, 2 env shadow
+    int mode;    // 0 radiance, 1 DL shadow, 2 env shadow, 3 BVH heatmap of radiance rays
     int nee;     // radiance pass: 0 none, 1 DL, 2 env
     const float* ext_rays;  // lux_trace_rays: rays given directly (n * 8 floats)
     uint32_t* ext_hits;     // and hits written directly (n * 5 words)
@@ -405,7 +409,7 @@ __global__ void __launch_bounds__(kTraceBlock, 7) k_trace(const __grid_constant_
     if (ext) {
         total = A.ext_n;
         cursor = A.ext_fetch;
-    } else if (MODE == 0) {
+    } else if (MODE == 0 || MODE == 3) {
         total = *(volatile int*)&A.W.ctr->count[A.bounce];
         cursor = &A.W.ctr->fetch_r[A.bounce];
     } else {
@@ -441,7 +445,7 @@ __global__ void __launch_bounds__(kTraceBlock, 7) k_trace(const __grid_constant_
                         tmax = MODE == 1 ? ry[3] : 1e16f;
                         L.pixel = __float_as_int(ry[7]);
                         L.iter = A.ext_iter;
-                    } else if (MODE == 0) {
+                    } else if (MODE == 0 || MODE == 3) {
                         int pid = A.W.queue[A.bounce & 1][r];
                         float4 a = A.W.s0[pid], b = A.W.s1[pid];
                         o = mk(a.x, a.y, a.z);
@@ -550,6 +554,12 @@ __global__ void __launch_bounds__(kTraceBlock, 7) k_trace(const __grid_constant_
                     bool hit = L.best.inst >= 0;
                     A.W.sh_hit[item] = make_float4(hit ? L.best.t : -1.0f, L.best.u, L.best.v, __int_as_float(L.best.inst));
                     A.W.sh_prim[item] = L.best.prim;
+                } else if (MODE == 3) {
+                    // drawBVH (src/kernels/draw_bvh.cu:33): color += count * 0.001 on every channel
+                    int pid = A.W.queue[A.bounce & 1][item];
+                    float4 c = A.W.s3[pid];
+                    const float h = float(L.work) * 0.001f;
+                    A.W.s3[pid] = make_float4(c.x + h, c.y + h, c.z + h, c.w);
                 } else {
                     A.W.sh_hit[item] = make_float4(L.best.inst >= 0 ? 1.0f : -1.0f, 0.0f, 0.0f, __int_as_float(-1));
                 }
@@ -564,14 +574,15 @@ __global__ void __launch_bounds__(kTraceBlock, 7) k_trace(const __grid_constant_
 }  // namespace
 
 int trace_grid_blocks(int mode) {
-    static int cached[3] = {0, 0, 0};
+    static int cached[4] = {0, 0, 0, 0};
     if (cached[mode] == 0) {
         int dev = 0, sms = 0, per = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (mode == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace<0>, kTraceBlock, 0);
         else if (mode == 1) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace<1>, kTraceBlock, 0);
-        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace<2>, kTraceBlock, 0);
+        else if (mode == 2) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace<2>, kTraceBlock, 0);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace<3>, kTraceBlock, 0);
         cached[mode] = sms * (per > 0 ? per : 1);
     }
     return cached[mode];
@@ -583,7 +594,8 @@ cudaError_t launch_trace(const DevScene& S, const DevWave& W, int bounce, int mo
     if (grid <= 0) grid = trace_grid_blocks(mode);
     if (mode == 0) k_trace<0><<<grid, kTraceBlock, 0, st>>>(A);
     else if (mode == 1) k_trace<1><<<grid, kTraceBlock, 0, st>>>(A);
-    else k_trace<2><<<grid, kTraceBlock, 0, st>>>(A);
+    else if (mode == 2) k_trace<2><<<grid, kTraceBlock, 0, st>>>(A);
+    else k_trace<3><<<grid, kTraceBlock, 0, st>>>(A);
     return cudaGetLastError();
 }
 

@@ -837,6 +837,30 @@ template <class T> V3<T> get_normal(const orc_scene& s, const lux_material_desc&
     return is.normal;
 }
 
+// The normal-map texel get_normal hands out (src/material_queries.cu:32-40); (0.5, 0.5, 1)
+// without a normal texture (:83-85).
+template <class T> V3<T> normal_map_texel(const orc_scene& s, const lux_material_desc& m, V2<T> uv) {
+    if (m.normal_tex < 0) return {T(0.5f), T(0.5f), T(1.0f)};
+    uv = apply_tt(uv, m.normal_tt);
+    T tx[4];
+    tex_fetch(s.texs[m.normal_tex], uv.x, uv.y, tx);
+    return {tx[0], tx[1], tx[2]};
+}
+
+// get_alpha (src/material_queries.cu:119-137)
+template <class T> T get_alpha(const orc_scene& s, const lux_material_desc& m, V2<T> uv) {
+    if (m.alpha_mode == LUX_ALPHA_OPAQUE) return T(1);
+    T alpha = T(m.alpha);
+    if (m.albedo_tex >= 0) {
+        uv = apply_tt(uv, m.albedo_tt);
+        T tx[4];
+        tex_fetch(s.texs[m.albedo_tex], uv.x, uv.y, tx);
+        alpha *= tx[3];
+    }
+    if (m.alpha_mode == LUX_ALPHA_MASK) return alpha >= T(m.alpha_cutoff) ? T(1) : T(0);
+    return alpha;
+}
+
 template <class T> void get_metallic_roughness(const orc_scene& s, const lux_material_desc& m, V2<T> uv, T& r, T& mt) {
     r = T(m.roughness);
     mt = T(m.metallic);
@@ -1206,6 +1230,24 @@ bool shade_path(const orc_scene& s, const lux_options& opt, int iter, int depth,
         V3<T> normal = get_normal(s, mat, is);
         T rough, metal;
         get_metallic_roughness(s, mat, is.uv, rough, metal);
+        if (opt.material_debug_mode) {
+            // render_material_debug_mode (src/material_debug_render.cu:3-26) replaces the
+            // colour and kills the path; shade_path.cu:154-164 skips the lighting
+            const int md = opt.material_debug_mode;
+            V3<T> c{T(0), T(0), T(0)};
+            if (md == 1) c = mc;
+            else if (md == 2) c = normal * T(0.5f) + V3<T>(T(0.5f), T(0.5f), T(0.5f));
+            else if (md == 3) c = normal_map_texel(s, mat, is.uv);
+            else if (md == 4) c = V3<T>(rough, rough, rough);
+            else if (md == 5) c = V3<T>(metal, metal, metal);
+            else if (md == 6) {
+                T a = get_alpha(s, mat, is.uv);
+                c = V3<T>(a, a, a);
+            }
+            path.color = c;
+            path.kill = true;
+            return false;
+        }
         V3<T> emission = get_emission(s, mat, is.uv);
         bool is_spec = rough < T(kSPEC_ROUGH);
         V3<T> nf = dot(-path.d, normal) < T(0) ? -normal : normal;
@@ -1431,6 +1473,7 @@ template <class T>
 void render_path(const orc_scene& s, const lux_options& opt, int iter, int pixel, V3<T>& color, double* st) {
     Path<T> p;
     int tdepth = opt.trace_depth > 0 ? opt.trace_depth : s.trace_depth;
+    if (opt.material_debug_mode) tdepth = 1;  // src/pathtrace.cu:107
     camera_ray(s, iter, pixel, tdepth, p);
     int depth = 0;
     bool nee = opt.direct_light_sampling || opt.env_importance_sampling;

@@ -347,7 +347,7 @@ ShadeableIntersection ch_direct_light(const ref_scene& R, const RHit& h) {
 
 void set_options(const lux_options* o) {
     DEV_OPTIONS.debug_bvh = false;
-    DEV_OPTIONS.material_debug_mode = 0;
+    DEV_OPTIONS.material_debug_mode = o ? o->material_debug_mode : 0;
     DEV_OPTIONS.color_mode = o ? o->color_mode : 2;
     DEV_OPTIONS.envmap_intensity = o ? o->envmap_intensity : 1.0f;
     DEV_OPTIONS.direct_light_sampling = o ? o->direct_light_sampling != 0 : false;
@@ -795,6 +795,7 @@ int ref_render(ref_scene* R, const lux_options* opt, int first_iter, int n_iter,
     set_options(opt);
     g_texs = &R->texs;
     int tdepth = opt->trace_depth > 0 ? opt->trace_depth : R->trace_depth;
+    if (opt->material_debug_mode) tdepth = 1;  // src/pathtrace.cu:107
     const lux_camera_desc& cd = R->cam;
     Camera c{};
     c.resolution = glm::ivec2(cd.width, cd.height);

@@ -138,3 +138,21 @@ def test_static_trace_limit_matches_header():
     text = open(HEADER).read()
     m = re.search(r"#define LUX_TRACE_STATIC_MAX_RAYS (\d+)", text)
     assert m and int(m.group(1)) == _ffi.TRACE_STATIC_MAX_RAYS
+
+
+def test_debug_views_validated_before_touching_a_device():
+    from luxion_b200._ffi import default_options
+    L = lx.lib()
+    s = lx.cornell36(8, 8)
+    h = C.c_void_p()
+    for kw, msg in ((dict(material_debug_mode=7), b"material_debug_mode"), (dict(material_debug_mode=-1), b"0..6"),
+                    (dict(debug_bvh=3), b"debug_bvh"), (dict(material_debug_mode=2, debug_bvh=1), b"exclusive")):
+        o = default_options(**kw)
+        assert L.lux_init(s.desc_ptr, C.byref(o), C.byref(h)) != 0
+        assert msg in L.lux_last_error()
+    # the job engine renders the production path only
+    o = default_options(debug_bvh=1)
+    scenes = (C.POINTER(_ffi.SceneDesc) * 1)(s.desc_ptr)
+    e = C.c_void_p()
+    assert L.lux_engine_create(scenes, 1, C.byref(o), None, C.byref(e)) == -5
+    assert b"debug views" in L.lux_last_error()

@@ -13,7 +13,7 @@ from luxion_b200 import cli
 def test_flags_as_the_reference_parses_them():
     a = cli.parse_args(["scene.glb", "-e", "sky.npy", "-i", "64", "-o", "out/name", "-dmis", "-emis", "-lock"])
     assert a == {"scene": "scene.glb", "envmap": "sky.npy", "iterations": 64, "output": "out/name",
-                 "dmis": True, "emis": True, "lock": True}
+                 "dmis": True, "emis": True, "lock": True, "debug_material": 0, "debug_bvh": False}
     assert cli.parse_args(["s", "--iterations", "3", "--envmap", "e", "--output", "o"])["iterations"] == 3
     assert cli.parse_args(["s"])["iterations"] == 5000          # the reference's default
     for bad, msg in ((["s", "-i"], "requires a number"), (["s", "-i", "0"], "invalid iteration count"),
@@ -23,6 +23,13 @@ def test_flags_as_the_reference_parses_them():
             cli.parse_args(bad)
     with pytest.raises(ValueError):
         cli.parse_args(["-dmis"])
+    # the debug views of the reference's ImGui panel (src/app/render_imgui.cpp:336-345)
+    assert cli.parse_args(["s", "-debug-material", "3"])["debug_material"] == 3
+    assert cli.parse_args(["s", "-debug-bvh"])["debug_bvh"] is True
+    for bad, msg in ((["s", "-debug-material"], "requires a number"), (["s", "-debug-material", "7"], "1..6"),
+                     (["s", "-debug-material", "1", "-debug-bvh"], "exclusive")):
+        with pytest.raises(ValueError, match=msg):
+            cli.parse_args(bad)
     assert cli.main([]) == 1
     assert cli.main(["missing.glb"]) == 1    # a scene file that cannot be read
 
@@ -41,6 +48,10 @@ def test_save_image_rule():
     assert list(out[0, 2]) == [ref(2.0), ref(0.5), ref(100.0)]
     assert list(out[1, 0]) == [ref(0.0), ref(1e-3), ref(0.2)]
     assert out[0, 2, 2] == 255 and out[1, 0, 0] == 0
+    # a material debug view is saved without ACES and gamma, still mirrored
+    raw = cli.to_png_bytes(img, 2, tonemap=False)
+    assert list(raw[0, 2]) == [255, int(np.float32(0.25) * np.float32(255)), 255]
+    assert list(raw[1, 0]) == [0, 0, int(np.float32(0.1) * np.float32(255))]
 
 
 def test_png_round_trip():

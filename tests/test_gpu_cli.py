@@ -35,3 +35,18 @@ def test_cli_envmap_and_emis():
         assert cli.main(["furnace", "-e", p, "-i", "2", "-o", out, "-emis"]) == 0
         png = cli.read_png(out + ".png")
     assert png.max() > 0
+
+
+def test_cli_material_debug_view():
+    with tempfile.TemporaryDirectory() as d:
+        out = os.path.join(d, "albedo")
+        assert cli.main(["cornell", "-i", "2", "-o", out, "-dmis", "-debug-material", "1"]) == 0
+        png = cli.read_png(out + ".png")
+    r = lx.Renderer(lx.cornell36(256, 256), default_options(direct_light_sampling=1, material_debug_mode=1))
+    r.render(1, 2)
+    img = r.image_sum()
+    r.close()
+    want = cli.to_png_bytes(img, 2, tonemap=False)
+    assert np.array_equal(png, want)
+    # the Cornell box's red wall albedo (0.63, 0.065, 0.05) shows as its raw value
+    assert (np.abs(want.reshape(-1, 3).astype(int) - [int(np.float32(0.63) * 255), 16, 12]).max(axis=1) <= 1).any()

@@ -369,3 +369,80 @@ def test_copy_image_device_equals_host_copy():
     stream.synchronize()
     assert np.array_equal(dev.cpu().numpy().view(np.uint32), r.image_sum().reshape(-1).view(np.uint32))
     r.close()
+
+
+# ---- debug views (src/material_debug_render.cu:3-26, src/kernels/draw_bvh.cu:6-35) -------------
+def debug_scene():
+    """A small random scene whose materials also carry normal maps, metallic-roughness textures
+    and alpha blending, so that every material debug view shows its channel."""
+    s = small_random_scene(seed=13, width=40, height=32)
+    d = s.desc
+    for k in range(d.num_materials):
+        m = d.materials[k]
+        if k % 2 == 1:
+            m.normal_tex = k % d.num_textures
+        if k % 3 == 1:
+            m.metallic_roughness_tex = (k + 1) % d.num_textures
+        if k == 2:
+            m.alpha_mode, m.alpha, m.albedo_tex = 2, 0.6, 0
+    return s
+
+
+@pytest.mark.parametrize("mode", range(1, 7))
+def test_material_debug_views_match_oracle(mode):
+    s = debug_scene()
+    opt = default_options(direct_light_sampling=1, env_importance_sampling=1, material_debug_mode=mode)
+    r = lx.Renderer(s, opt)
+    r.render(3, 4)
+    a = r.image_sum()
+    rgba = r.rgba8()
+    st = r.stats()
+    r.close()
+    b, sb = ol.OracleScene(s).render(opt, 3, 4)
+    frac, relmse = image_parity(a, b)
+    assert frac >= PIXEL_FRAC and relmse <= RELMSE_TOL, (frac, relmse)
+    assert st["path_bounces"] == 4 * s.width * s.height  # trace depth 1
+    assert st["rays_radiance"] == sb[0] and st["rays_shadow"] == sb[1]
+    # the display shows the mean without tone map or gamma (src/kernels/image_kernels.cu:20-33)
+    p = a * np.float32(1.0 / 4.0)
+    want = np.clip((p.astype(np.float64) * 255.0).astype(np.int64), 0, 255)
+    assert np.abs(rgba[..., :3].astype(np.int64) - want).max() <= 1
+
+
+def test_bvh_heatmap():
+    s = debug_scene()
+    opt = default_options(direct_light_sampling=1, env_importance_sampling=1, debug_bvh=1)
+    r = lx.Renderer(s, opt)
+    r.render(1, 1)
+    a = r.image_sum()
+    st = r.stats()
+    r.reset()
+    r.render(1, 1)
+    again = r.image_sum()
+    r.close()
+    assert np.array_equal(a.view(np.uint32), again.view(np.uint32))  # deterministic
+    assert st["rays_radiance"] == s.width * s.height and st["rays_shadow"] == 0
+    assert np.array_equal(a[..., 0], a[..., 1]) and np.array_equal(a[..., 0], a[..., 2])
+    counts = np.rint(a[..., 0] / np.float32(0.001)).astype(np.int64)
+    assert np.array_equal((counts.astype(np.float32) * np.float32(0.001)), a[..., 0])
+    assert counts.min() >= 1  # every ray visits at least the TLAS root
+    # rays that hit geometry do more traversal work than rays that escape (hit mask from the
+    # oracle's camera rays; they are jittered with another seed, which moves only silhouettes)
+    o = ol.OracleScene(s)
+    pix = np.arange(s.width * s.height, dtype=np.int32)
+    hits = o.trace(ol.camera_paths_to_rays(o.camera_rays(pix, 1)), 0, 1)
+    hit = (hits[:, 1] != 0xFFFFFFFF).reshape(s.height, s.width)
+    assert hit.any() and (~hit).any()
+    assert counts[hit].mean() > counts[~hit].mean()
+
+
+def test_debug_option_validation():
+    s = debug_scene()
+    for kw, msg in ((dict(material_debug_mode=7), b"material_debug_mode"), (dict(debug_bvh=2), b"debug_bvh"),
+                    (dict(material_debug_mode=1, debug_bvh=1), b"exclusive")):
+        with pytest.raises(lx.LuxError) as e:
+            lx.Renderer(s, default_options(**kw))
+        assert msg in str(e.value).encode() or msg in lx.lib().lux_last_error()
+    # the job engine renders the production path only
+    with pytest.raises(lx.LuxError, match="debug views"):
+        lx.Engine([s], default_options(material_debug_mode=1))

@@ -48,3 +48,32 @@ def test_cornell_render_matches_reference():
     a, _ = ol.OracleScene(s).render(opt, 1, 3)
     b, _ = ol.RefScene(s).render(opt, 1, 3)
     assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def scene_debug(seed=5):
+    """scene_rand with normal maps, metallic-roughness textures and an alpha-blended material,
+    so every material debug view has something to show."""
+    s = scene_rand(seed=seed)
+    d = s.desc
+    for k in range(d.num_materials):
+        m = d.materials[k]
+        if k % 2 == 1:
+            m.normal_tex = k % d.num_textures
+        if k % 3 == 1:
+            m.metallic_roughness_tex = (k + 1) % d.num_textures
+        if k == 2:
+            m.alpha_mode, m.alpha, m.albedo_tex = 2, 0.6, 0
+    return s
+
+
+@pytest.mark.parametrize("mode", range(1, 7))
+def test_material_debug_views_match_reference(mode):
+    """render_material_debug_mode (src/material_debug_render.cu:3-26) through the reference's own
+    shadePath at trace depth 1 (src/pathtrace.cu:107)."""
+    s = scene_debug()
+    opt = default_options(direct_light_sampling=1, env_importance_sampling=1, material_debug_mode=mode)
+    a, sa = ol.OracleScene(s).render(opt, 3, 2)
+    b, sb = ol.RefScene(s).render(opt, 3, 2)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert np.array_equal(sa, sb)
+    assert sa[2] == 2 * s.width * s.height  # one bounce per sample
