@@ -431,7 +431,7 @@ def main():
         e_ms, e_rays = [], 0.0
         h2d = 0
         img_host = np.empty((H, W, 3), np.float32)
-        for k in range(2):
+        for k in range(3):  # the fastest of three cold runs: host-side init varies from run to run
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             rr = lx.Renderer(scene, opt)
