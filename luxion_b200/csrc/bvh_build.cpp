@@ -226,7 +226,7 @@ void build_binary(const float* boxes, int n, Binary& B) {
 // 1e-4 of its largest extent (plus 1e-7 of its coordinate magnitude), at least 1.27 % of a
 // quantisation step on every axis, and every child plane is rounded outward by a further 1 %
 // of a step. Either margin dominates the rounding error of the device slab test: at most
-// 2^-9 of a step beyond a relative 2^-19 of the plane distance, which the device widens.
+// 2^-9 of a step beyond a relative 2^-17 of the plane distance, which the device widens.
 void encode_node(BVH8Node& N, const Box& nb, const Box* cbox, const bool* used) {
     double mext = 0.0, mabs = 0.0;
     for (int a = 0; a < 3; ++a) {

@@ -21,8 +21,8 @@
 //    for bit on the same rays; equal t is resolved toward the lowest (instance, primitive);
 //  * alpha mask / blend any-hit (optix_triangle.cu:317-366) is evaluated on candidate hits of
 //    instances whose material is not opaque.
-// Box tests are conservative: child boxes are quantised outward at build time and the slab
-// interval is widened by a relative 2^-19, so no triangle the exact test accepts is skipped.
+// Box tests are conservative: child boxes are quantised outward at build time and a child is
+// entered while tnear <= tfar * (1 + 2^-17), so no triangle the exact test accepts is skipped.
 
 #include "device_scene.h"
 #include "device_math.cuh"
@@ -46,8 +46,10 @@ constexpr uint32_t kRecMask = 0xffffffu;
 // traversing nodes (the postponement of Ylitie et al. 2017); 4 and a refill threshold of 24
 // lanes were the fastest of the values tried on the 1M-triangle 1080p workload
 constexpr int kPostpone = 4;
-constexpr float kLo = 1.0f - 1.0f / 524288.0f;
-constexpr float kHi = 1.0f + 1.0f / 524288.0f;
+// Slab acceptance tnear <= tfar * kWiden (tnear >= 0): a relative margin of 2^-17, far above
+// the few-ulp rounding of the plane distances.
+constexpr float kWiden = 1.0f + 1.0f / 131072.0f;
+static_assert(kMaxLeafPrims == 1, "visit_node marks one triangle per leaf slot");
 
 struct TRay {
     f3 o, d, idir;
@@ -109,13 +111,12 @@ LUX_DI void visit_node(const uint4* __restrict__ nodes, uint32_t ni, const TRay&
         float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
         float tf = fminf(fminf(tfx, tfy), fminf(tfz, tmax));
         uint32_t meta = ((s < 4 ? w1.z : w1.w) >> (8 * b)) & 0xffu;
-        bool hit = (meta != 0u) && (tn * kLo <= tf * kHi);
+        bool hit = (meta != 0u) && (tn <= tf * kWiden);
         if (hit) {
             if (meta & 0x80u) {
                 keys |= 1u << (uint32_t(s) ^ r.oct);
             } else {
-                uint32_t cnt = meta >> 5, off = meta & 31u;
-                trimask |= ((1u << cnt) - 1u) << off;
+                trimask |= 1u << (meta & 31u);  // the slot's one triangle, at its record offset
             }
         }
     }
