@@ -13,9 +13,11 @@
 //   imask      u8    bit s set: slot s holds an internal child
 //   child_base u32   index of the first internal child; internal children are stored
 //                    contiguously in slot order
-//   tri_base   u32   first primitive record of the leaf slots
-//   meta[8]    u8    per slot: 0 empty; 0x80|rank internal; (count<<5)|offset leaf with
-//                    count in 1..kMaxLeafPrims primitives starting at tri_base+offset
+//   tri_base   u32   first primitive record of the leaf slots; each leaf slot holds one
+//                    primitive, stored in slot order (record = tri_base + rank of the slot
+//                    among the leaf slots)
+//   meta[8]    u8    meta[0]: bit s set: slot s is a leaf; meta[1..7] zero. A slot in neither
+//                    imask nor meta[0] is empty
 //   q{lo,hi}{x,y,z}[8] u8  child boxes: lo = p + q*scale (rounded outward at build time)
 // Child slots are assigned by the octant of the child centroid around the node centre, so a
 // ray visits slots in the order (slot ^ ray_octant) to go near-to-far.

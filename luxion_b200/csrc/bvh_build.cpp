@@ -370,22 +370,19 @@ void build_bvh8(const float* boxes, int n, BVH8Build& out) {
         encode_node(N, bn.box, cbox, slot_used);
         N.child_base = uint32_t(out.nodes.size());
         N.tri_base = uint32_t(out.prim_order.size());
-        int rank = 0;
         for (int s = 0; s < 8; ++s) {
             int c = child_at_slot[s];
             if (c < 0) continue;
             const BNode& cn = B.nodes[c];
             out.sah_cost += cn.box.area() / root_area;
             if (cn.left < 0 || cn.count <= kMaxLeafPrims) {
-                int off = int(out.prim_order.size()) - int(N.tri_base);
+                // one record per leaf slot, in slot order: the record is the slot's rank
                 for (int k = cn.begin; k < cn.begin + cn.count; ++k) out.prim_order.push_back(B.order[k]);
-                N.meta[s] = uint8_t((cn.count << 5) | off);
+                N.meta[0] = uint8_t(N.meta[0] | (1u << s));
             } else {
                 N.imask |= uint8_t(1u << s);
-                N.meta[s] = uint8_t(0x80 | rank);
                 out.nodes.push_back(BVH8Node());
                 q.push_back({c, int(out.nodes.size()) - 1, it.level + 1});
-                ++rank;
             }
         }
         out.nodes[it.out_index] = N;

@@ -41,7 +41,7 @@ constexpr uint32_t kTagNode = 0u;
 constexpr uint32_t kTagTri = 1u << 30;
 constexpr uint32_t kTagInst = 2u << 30;
 constexpr uint32_t kTagMarker = 3u << 30;
-constexpr uint32_t kRecMask = 0xffffffu;
+constexpr uint32_t kRecMask = 0xffu;
 // fewer lanes than this with triangles to test: push the triangle groups and keep
 // traversing nodes (the postponement of Ylitie et al. 2017); 4 and a refill threshold of 24
 // lanes were the fastest of the values tried on the 1M-triangle 1080p workload
@@ -71,9 +71,11 @@ LUX_DI TRay make_ray(f3 o, f3 d) {
 LUX_DI float ubyte_biased(uint32_t w, int s) { return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7504u | (uint32_t(s) << 4))); }
 
 // Intersect the 8 child boxes of node ni. Returns internal-child hits as a key mask
-// (bit (slot ^ oct)), the leaf primitive mask (bit offset), child_base and tri_base.
+// (bit slot ^ oct), leaf hits as a slot mask, the node's leaf-slot mask, child_base and
+// tri_base.
 LUX_DI void visit_node(const uint4* __restrict__ nodes, uint32_t ni, const TRay& r, float tmax, uint32_t& keys,
-                       uint32_t& imask, uint32_t& child_base, uint32_t& tri_base, uint32_t& trimask) {
+                       uint32_t& imask, uint32_t& child_base, uint32_t& tri_base, uint32_t& trimask,
+                       uint32_t& leafmask) {
     const uint4* n = nodes + size_t(ni) * 5;
     uint4 w0 = __ldg(n + 0), w1 = __ldg(n + 1), w2 = __ldg(n + 2), w3 = __ldg(n + 3), w4 = __ldg(n + 4);
     float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
@@ -97,8 +99,7 @@ LUX_DI void visit_node(const uint4* __restrict__ nodes, uint32_t ni, const TRay&
     uint32_t nx0 = fx ? w3.z : w2.x, nx1 = fx ? w3.w : w2.y, fx0 = fx ? w2.x : w3.z, fx1 = fx ? w2.y : w3.w;
     uint32_t ny0 = fy ? w4.x : w2.z, ny1 = fy ? w4.y : w2.w, fy0 = fy ? w2.z : w4.x, fy1 = fy ? w2.w : w4.y;
     uint32_t nz0 = fz ? w4.z : w3.x, nz1 = fz ? w4.w : w3.y, fz0 = fz ? w3.x : w4.z, fz1 = fz ? w3.y : w4.w;
-    keys = 0;
-    trimask = 0;
+    uint32_t hits = 0;
 #pragma unroll
     for (int s = 0; s < 8; ++s) {
         const int b = s & 3;
@@ -110,16 +111,16 @@ LUX_DI void visit_node(const uint4* __restrict__ nodes, uint32_t ni, const TRay&
               tfz = fmaf(ubyte_biased(wfz, b), az, bz);
         float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
         float tf = fminf(fminf(tfx, tfy), fminf(tfz, tmax));
-        uint32_t meta = ((s < 4 ? w1.z : w1.w) >> (8 * b)) & 0xffu;
-        bool hit = (meta != 0u) && (tn <= tf * kWiden);
-        if (hit) {
-            if (meta & 0x80u) {
-                keys |= 1u << (uint32_t(s) ^ r.oct);
-            } else {
-                trimask |= 1u << (meta & 31u);  // the slot's one triangle, at its record offset
-            }
-        }
+        if (tn <= tf * kWiden) hits |= 1u << s;
     }
+    leafmask = w1.z & 0xffu;
+    hits &= imask | leafmask;
+    trimask = hits & leafmask;
+    uint32_t ih = hits & imask;  // to key order: bit s moves to bit s ^ oct
+    if (r.oct & 1) ih = ((ih & 0x55u) << 1) | ((ih >> 1) & 0x55u);
+    if (r.oct & 2) ih = ((ih & 0x33u) << 2) | ((ih >> 2) & 0x33u);
+    if (r.oct & 4) ih = ((ih & 0x0Fu) << 4) | ((ih >> 4) & 0x0Fu);
+    keys = ih;
 }
 
 struct Best {
@@ -208,7 +209,8 @@ struct Lane {
     float tmax;
     Best best;
     uint2 g;            // node group: x = first internal child, y = imask << 8 | remaining hit keys
-    uint2 t;            // leaf group: x = first record, y = tag (kTagTri / kTagInst) | record mask
+    uint2 t;            // leaf group: x = first record, y = tag (kTagTri / kTagInst) | leaf-slot
+                        // mask << 8 | remaining hit slots
     int sp;             // stack depth
     int inst;           // current instance (-1 in the TLAS)
     int inst_flags;
@@ -271,22 +273,24 @@ struct Tracer {
         uint32_t imask = L.g.y >> 8;
         uint32_t child = L.g.x + __popc(imask & ((1u << slot) - 1u));
         if (keys) push(L, make_uint2(L.g.x, (imask << 8) | keys));
-        uint32_t nkeys, nimask, cbase, tbase, tmask;
-        visit_node(S.nodes, child, L.cur, limit(L), nkeys, nimask, cbase, tbase, tmask);
+        uint32_t nkeys, nimask, cbase, tbase, tmask, lmask;
+        visit_node(S.nodes, child, L.cur, limit(L), nkeys, nimask, cbase, tbase, tmask, lmask);
         if (MODE == 3) ++L.work;
         L.g = make_uint2(cbase, (nimask << 8) | nkeys);
         if (tmask) {
-            if (L.inst >= 0) L.t = make_uint2(L.inst_prim_base + tbase, kTagTri | tmask);
-            else L.t = make_uint2(tbase, kTagInst | tmask);
+            if (L.inst >= 0) L.t = make_uint2(L.inst_prim_base + tbase, kTagTri | (lmask << 8) | tmask);
+            else L.t = make_uint2(tbase, kTagInst | (lmask << 8) | tmask);
         }
     }
 
     // Triangle phase: test the lowest triangle of the leaf group.
     LUX_DI void test_one(Lane& L) {
         uint32_t m = L.t.y & kRecMask;
+        const uint32_t lm = (L.t.y >> 8) & 0xffu;
         int k = __ffs(m) - 1;
         m &= m - 1;
-        L.t.y = m ? (kTagTri | m) : 0u;
+        L.t.y = m ? (kTagTri | (lm << 8) | m) : 0u;
+        k = __popc(lm & ((1u << k) - 1u));  // the slot's record: its rank among the leaf slots
         float t, u, v;
         int prim;
         if (MODE == 3) ++L.work;
@@ -308,14 +312,17 @@ struct Tracer {
     // group and the rest of the leaf group wait on the stack under a marker.
     LUX_DI void enter(Lane& L) {
         uint32_t m = L.t.y & kRecMask;
+        const uint32_t lm = (L.t.y >> 8) & 0xffu;
         int k = __ffs(m) - 1;
         m &= m - 1;
+        const int slot_k = k;
+        k = __popc(lm & ((1u << slot_k) - 1u));
         // the instance's leaf record: transform and BLAS root in one dependent 64-byte load
         const float4* q = S.tlas_leaf + size_t(L.t.x + uint32_t(k)) * 4;
         const float4 r0 = __ldg(q), r1 = __ldg(q + 1), r2 = __ldg(q + 2);
         const uint4 e = __ldg(reinterpret_cast<const uint4*>(q + 3));
         if (L.g.y & 0xffu) push(L, L.g);
-        if (m) push(L, make_uint2(L.t.x, kTagInst | m));
+        if (m) push(L, make_uint2(L.t.x, kTagInst | (lm << 8) | m));
         push(L, make_uint2(0u, kTagMarker));
         const float Minv[12] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w};
         L.cur = make_ray(xform(Minv, L.wo, 1.0f), xform(Minv, L.wd, 0.0f));
