@@ -366,6 +366,22 @@ bool light_tables(const lux_scene_desc& d, const float* env, std::vector<int>& e
     return true;
 }
 
+// Guide table of one CDF (select_from_cdf_guided): g[j] = first i with cdf[i] >= j/m, or n-1.
+void cdf_guide(const float* cdf, int n, int m, int* g) {
+    int i = 0;
+    for (int j = 0; j <= m; ++j) {
+        const float t = float(j) / float(m);  // exact: m is a power of two
+        while (i < n - 1 && cdf[i] < t) ++i;
+        g[j] = i;
+    }
+}
+
+int pow2_at_least(int v) {
+    int m = 1;
+    while (m < v && m < (1 << 16)) m <<= 1;
+    return m;
+}
+
 }  // namespace
 
 int lux::build_host_scene(const lux_scene_desc& d, const lux_options& opt, std::vector<DevTex>& texs,
@@ -685,6 +701,20 @@ int lux::build_host_scene(const lux_scene_desc& d, const lux_options& opt, std::
         env_ok = light_tables<float>(d, envt, H.emissive, H.emissive_prefix, tri_prefix, H.total_area, H.marginal,
                                      H.conditional);
     if (!env_ok) return fail(LUX_ERR_INVALID, "environment map has no emission");
+    if (d.env_data) {
+        // about one marginal entry and four conditional entries per guide cell
+        const int W = d.env_width, Hh = d.env_height;
+        H.guide_marg = pow2_at_least(Hh);
+        H.guide_cond = pow2_at_least(std::max(1, W / 4));
+        H.marginal_guide.resize(size_t(H.guide_marg) + 1);
+        cdf_guide(H.marginal.data(), Hh, H.guide_marg, H.marginal_guide.data());
+        H.conditional_guide.resize(size_t(H.guide_cond + 1) * Hh);
+        parallel_chunks(Hh, [&](int y0, int y1) {
+            for (int y = y0; y < y1; ++y)
+                cdf_guide(H.conditional.data() + size_t(y) * W, W, H.guide_cond,
+                          H.conditional_guide.data() + size_t(y) * (H.guide_cond + 1));
+        });
+    }
     H.tri_off.clear();
     H.tri_prefix.clear();
     for (int e : H.emissive) {

@@ -119,6 +119,23 @@ LUX_DI int select_from_cdf(const float* __restrict__ cdf, int size, float xi) {
     return low;
 }
 
+// select_from_cdf over a bracket from a guide table. guide[j] = select_from_cdf(cdf, size, j/m)
+// for j in 0..m (m a power of two, so j = floor(xi * m) and j/m are exact). The answer is
+// monotone in xi, so for xi in [j/m, (j+1)/m] it lies in [guide[j], guide[j+1]], and the same
+// first-index-not-below-xi search over that bracket returns the same index with far fewer
+// dependent loads.
+LUX_DI int select_from_cdf_guided(const float* __restrict__ cdf, const int* __restrict__ guide, int m, float xi) {
+    int j = int(xi * float(m));
+    j = j < 0 ? 0 : (j > m - 1 ? m - 1 : j);
+    int low = __ldg(guide + j), high = __ldg(guide + j + 1);
+    while (low < high) {
+        int mid = low + (high - low) / 2;
+        if (__ldg(cdf + mid) < xi) low = mid + 1;
+        else high = mid;
+    }
+    return low;
+}
+
 // OptiX any-hit hash (src/optixshaders/optix_triangle.cu:41-49)
 LUX_HDI uint32_t hash_u32(uint32_t x) {
     x ^= x >> 16;

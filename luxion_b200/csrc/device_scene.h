@@ -87,6 +87,9 @@ struct DevScene {
     float total_area;
     const float* marginal;
     const float* conditional;
+    const int* marginal_guide;     // guide_marg + 1 entries (select_from_cdf_guided)
+    const int* conditional_guide;  // guide_cond + 1 entries per row
+    int guide_marg, guide_cond;
     int env_w, env_h;
     unsigned long long env_tex;
     int has_env;

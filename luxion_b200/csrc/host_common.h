@@ -96,6 +96,8 @@ struct HostScene {
     std::vector<DevMaterial> mats;
     std::vector<int> emissive;        // emissive instances
     std::vector<float> emissive_prefix, tri_prefix, marginal, conditional;
+    std::vector<int> marginal_guide, conditional_guide;  // guide tables of the HDRI CDFs
+    int guide_marg = 0, guide_cond = 0;
     std::vector<int> tri_off;
     float total_area = 0.0f;
     int env_w = 0, env_h = 0;
@@ -138,6 +140,13 @@ int upload_scene_lights(Owner* C, const HostScene& H, DevScene& S) {
         S.marginal = f;
         if ((rc = C->up(&f, H.conditional.data(), H.conditional.size()))) return rc;
         S.conditional = f;
+        int* g = nullptr;
+        if ((rc = C->up(&g, H.marginal_guide.data(), H.marginal_guide.size()))) return rc;
+        S.marginal_guide = g;
+        if ((rc = C->up(&g, H.conditional_guide.data(), H.conditional_guide.size()))) return rc;
+        S.conditional_guide = g;
+        S.guide_marg = H.guide_marg;
+        S.guide_cond = H.guide_cond;
         S.env_w = H.env_w;
         S.env_h = H.env_h;
         S.env_tex = H.env_tex;

@@ -429,13 +429,14 @@ LUX_DI f3 light_sample(const DevScene& S, const DevOptions& O, int iter, int pix
     if (O.env) {
         float rnd = rng.u01();
         const int H = S.env_h, W = S.env_w;
-        int mg = select_from_cdf(S.marginal, H, rnd);
+        int mg = select_from_cdf_guided(S.marginal, S.marginal_guide, S.guide_marg, rnd);
         float lower = (mg == 0) ? 0.0f : __ldg(S.marginal + mg - 1);
         float upper = __ldg(S.marginal + mg);
         float den = upper - lower;
         float off = (den > 1e-10f) ? (rnd - lower) / den : 0.0f;
         off = gclamp(off, 0.0f, 1.0f);
-        int cn = select_from_cdf(S.conditional + size_t(mg) * W, W, off);
+        int cn = select_from_cdf_guided(S.conditional + size_t(mg) * W,
+                                        S.conditional_guide + size_t(mg) * (S.guide_cond + 1), S.guide_cond, off);
         float u = (float(cn) + 0.5f) / float(W);
         float v = (float(mg) + 0.5f) / float(H);
         float phi = float(double(u) * 2.0 * double(kPI) - double(kPI));
