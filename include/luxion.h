@@ -421,8 +421,16 @@ typedef struct lux_random_scene_params {
 void lux_default_random_scene_params(lux_random_scene_params* p);
 lux_host_scene* lux_scene_random(const lux_random_scene_params* p);
 
-/* Furnace: a closed unit sphere (Lambert albedo 1) inside a constant environment of 1. */
+/* Furnace: a closed unit icosphere (vertex normals on) under a constant environment of 1,
+ * made of smooth white metal (metallic 1, roughness 0.01, base colour 1, so Schlick F = 1). */
 lux_host_scene* lux_scene_furnace(int width, int height, int subdiv);
+/* The same furnace with the sphere made of *mat; vertex_normals 0 drops the vertex normals, so
+ * the sphere shades with its geometric (facet) normals and stays exactly convex. */
+lux_host_scene* lux_scene_furnace_material(int width, int height, int subdiv, const lux_material_desc* mat,
+                                           int vertex_normals);
+/* The material the procedural scenes start from: the reference glTF defaults for base colour
+ * 1, roughness 1, metallic 0, ior 1.55 (src/scene/scene_load_gltf.cpp:85-89,177). */
+void lux_default_material(lux_material_desc* m);
 
 /* A pinhole camera at pos looking at look (world up +y) with vertical field of view fovy_deg
  * at width x height, set up as the reference's scene loader does from a camera's position,

@@ -71,6 +71,8 @@ SIGNATURES = {
     "lux_default_random_scene_params": (None, [C.POINTER(RandomSceneParams)]),
     "lux_scene_random": (_P, [C.POINTER(RandomSceneParams)]),
     "lux_scene_furnace": (_P, [C.c_int, C.c_int, C.c_int]),
+    "lux_scene_furnace_material": (_P, [C.c_int, C.c_int, C.c_int, C.POINTER(_ffi.MaterialDesc), C.c_int]),
+    "lux_default_material": (None, [C.POINTER(_ffi.MaterialDesc)]),
     "lux_scene_get_desc": (C.POINTER(SceneDesc), [_P]),
     "lux_scene_instanced_tris": (C.c_int64, [_P]),
     "lux_scene_destroy": (None, [_P]),
@@ -164,8 +166,21 @@ def random_scene(**kw) -> HostScene:
     return HostScene(lib().lux_scene_random(C.byref(p)))
 
 
-def furnace(width: int = 64, height: int = 64, subdiv: int = 16) -> HostScene:
-    return HostScene(lib().lux_scene_furnace(width, height, subdiv))
+def furnace(width: int = 64, height: int = 64, subdiv: int = 16, vertex_normals: bool = True,
+            **material) -> HostScene:
+    """White furnace: a unit icosphere under a constant environment of 1. Without material
+    keywords the sphere is smooth white metal (lux_scene_furnace); keywords (color, roughness,
+    metallic, ior, transmission, ...) override the reference glTF default material."""
+    if not material and vertex_normals:
+        return HostScene(lib().lux_scene_furnace(width, height, subdiv))
+    m = _ffi.MaterialDesc()
+    lib().lux_default_material(C.byref(m))
+    for k, v in material.items():
+        if k == "color":
+            m.color[:] = [float(x) for x in v]
+        else:
+            setattr(m, k, v)
+    return HostScene(lib().lux_scene_furnace_material(width, height, subdiv, C.byref(m), 1 if vertex_normals else 0))
 
 
 # ---- renderer -------------------------------------------------------------------------------

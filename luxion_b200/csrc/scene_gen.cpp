@@ -8,7 +8,8 @@
 //   * random instanced scene: icospheres and displaced grids with random transforms,
 //     random uber-shader materials, value-noise base-colour textures and an HDRI made of a
 //     log-normal sky and a Gaussian sun lobe.
-//   * white furnace: a smooth white metal sphere under a constant environment of 1.
+//   * white furnace: a sphere under a constant environment of 1, by default smooth white
+//     metal; any material can be given (a Lambert-like albedo-1 dielectric, rough GGX metal).
 // Camera conventions follow the glTF loader (scene_load_gltf.cpp:465-500): view = -z of the
 // camera frame, pixelLength = 2*tan(fovy/2)*(aspect, 1)/resolution.
 
@@ -676,14 +677,20 @@ lux_host_scene* lux_scene_random(const lux_random_scene_params* prm) {
 }
 
 lux_host_scene* lux_scene_furnace(int width, int height, int subdiv) {
-    auto s = std::make_unique<lux_host_scene>();
-    std::memset(&s->desc, 0, sizeof(s->desc));
-    add_icosphere(*s, std::max(2, subdiv), 1u, 0.0);
     lux_material_desc m = default_material();
     m.metallic = 1.0f;
     m.roughness = 0.01f;
-    m.color[0] = m.color[1] = m.color[2] = 1.0f;
-    s->mats.push_back(m);
+    return lux_scene_furnace_material(width, height, subdiv, &m, 1);
+}
+
+lux_host_scene* lux_scene_furnace_material(int width, int height, int subdiv, const lux_material_desc* mat,
+                                           int vertex_normals) {
+    if (!mat) return nullptr;
+    auto s = std::make_unique<lux_host_scene>();
+    std::memset(&s->desc, 0, sizeof(s->desc));
+    add_icosphere(*s, std::max(2, subdiv), 1u, 0.0);
+    if (!vertex_normals) s->nrm.back().clear();
+    s->mats.push_back(*mat);
     s->insts.push_back(make_instance(0, 0, identity()));
     const int W = 64, H = 32;
     s->env32.assign(size_t(W) * H * 4, 1.0f);
@@ -695,6 +702,10 @@ lux_host_scene* lux_scene_furnace(int width, int height, int subdiv) {
     s->desc.trace_depth = 8;
     s->finalize();
     return s.release();
+}
+
+void lux_default_material(lux_material_desc* m) {
+    if (m) *m = default_material();
 }
 
 const lux_scene_desc* lux_scene_get_desc(const lux_host_scene* s) { return s ? &s->desc : nullptr; }

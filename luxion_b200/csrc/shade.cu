@@ -21,6 +21,8 @@
 #include "launch.h"
 
 #include <algorithm>
+#include <map>
+#include <mutex>
 
 namespace lux {
 namespace {
@@ -946,11 +948,17 @@ __global__ void k_tex_ext(unsigned long long t, const float* uv, int n, float* o
 
 }  // namespace
 
+// Grid of the shading kernels: SMs x resident blocks per SM, cached per device ordinal under a
+// lock, as trace_grid_blocks is.
 int shade_grid_blocks() {
-    static int cached = 0;
+    static std::mutex mu;
+    static std::map<int, int> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
+    int& cached = cache[dev];
     if (cached == 0) {
-        int dev = 0, sms = 0, per = 0;
-        cudaGetDevice(&dev);
+        int sms = 0, per = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         int per_jobs = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_shade<false, false>, kShadeBlock, 0);

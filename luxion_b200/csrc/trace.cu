@@ -29,6 +29,10 @@
 #include "bvh8.h"
 #include "launch.h"
 
+#include <array>
+#include <map>
+#include <mutex>
+
 namespace lux {
 
 namespace {
@@ -591,19 +595,26 @@ __global__ void __launch_bounds__(kTraceBlock, 7) k_trace(const __grid_constant_
 
 }  // namespace
 
+// Persistent grid of each traversal kind: SMs x resident blocks per SM. The answer depends on
+// the device, so it is cached per device ordinal, under a lock (contexts on several devices and
+// several host threads ask for it).
 int trace_grid_blocks(int mode) {
-    static int cached[4] = {0, 0, 0, 0};
-    if (cached[mode] == 0) {
-        int dev = 0, sms = 0, per = 0;
-        cudaGetDevice(&dev);
+    static std::mutex mu;
+    static std::map<int, std::array<int, 4>> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
+    int& cached = cache[dev][mode];
+    if (cached == 0) {
+        int sms = 0, per = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (mode == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace<0>, kTraceBlock, 0);
         else if (mode == 1) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace<1>, kTraceBlock, 0);
         else if (mode == 2) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace<2>, kTraceBlock, 0);
         else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace<3>, kTraceBlock, 0);
-        cached[mode] = sms * (per > 0 ? per : 1);
+        cached = sms * (per > 0 ? per : 1);
     }
-    return cached[mode];
+    return cached;
 }
 
 cudaError_t launch_trace(const DevScene& S, const DevWave& W, int bounce, int mode, int nee, cudaStream_t st,
