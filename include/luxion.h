@@ -182,13 +182,32 @@ typedef struct lux_options {
 } lux_options;
 
 typedef struct lux_ctx lux_ctx;
+typedef struct lux_scene lux_scene;
 
 /* Fill *opt with the reference defaults (include/pathtrace/pathtracer_options.h:3-11). */
 void lux_default_options(lux_options* opt);
 
 /* pathtraceInit: upload the scene, build the acceleration structure and the light CDFs,
- * allocate every per-path buffer. */
+ * allocate every per-path buffer. The context owns the scene it built. */
 int lux_init(const lux_scene_desc* scene, const lux_options* opt, lux_ctx** out);
+
+/* A resident scene: geometry, BVH, materials, textures and light CDFs on one device, built
+ * once. The reference does this work at load, before the first pathtraceInit: mesh uploads and
+ * acceleration builds in main() (src/main.cpp:199-274) and the light precompute
+ * (src/scene/scene_precompute.cpp:22-124). Of the options only device, texture_storage and
+ * precision shape the build; every context made on the scene must use the same three. */
+int lux_scene_create(const lux_scene_desc* scene, const lux_options* opt, lux_scene** out);
+/* pathtraceInit on a resident scene (src/pathtrace/pathtrace_buffers.cu:21-140): allocate only
+ * the per-pixel and per-path state for `camera` (any resolution; NULL = the description's
+ * camera) and take the trace depth from opt (0 = the description's). No scene work is done, so
+ * the reference's pathtraceFree(); pathtraceInit() on every camera or option reset
+ * (src/app/render_loop.cpp:122-126) costs allocations only. The context holds a reference to
+ * the scene. */
+int lux_init_on_scene(lux_scene* scene, const lux_camera_desc* camera, const lux_options* opt, lux_ctx** out);
+/* Drop the caller's reference: the scene is freed once no context uses it. NULL is accepted. */
+int lux_scene_free(lux_scene* scene);
+/* Device bytes the scene holds (geometry, BVH, tables, textures). */
+int64_t lux_scene_device_bytes(const lux_scene* scene);
 
 /* pathtrace: render one sample per pixel. iter is 1-based and seeds the RNG exactly like
  * the reference (include/common.h:38-47). The sample is added to the FP32 accumulation

@@ -34,6 +34,10 @@ _P = C.c_void_p
 SIGNATURES = {
     "lux_default_options": (None, [C.POINTER(Options)]),
     "lux_init": (C.c_int, [C.POINTER(SceneDesc), C.POINTER(Options), C.POINTER(_P)]),
+    "lux_scene_create": (C.c_int, [C.POINTER(SceneDesc), C.POINTER(Options), C.POINTER(_P)]),
+    "lux_init_on_scene": (C.c_int, [_P, C.POINTER(CameraDesc), C.POINTER(Options), C.POINTER(_P)]),
+    "lux_scene_free": (C.c_int, [_P]),
+    "lux_scene_device_bytes": (C.c_int64, [_P]),
     "lux_render_iter": (C.c_int, [_P, C.c_int, _P]),
     "lux_render": (C.c_int, [_P, C.c_int, C.c_int]),
     "lux_copy_image": (C.c_int, [_P, c_float_p]),
@@ -184,17 +188,66 @@ def furnace(width: int = 64, height: int = 64, subdiv: int = 16, vertex_normals:
 
 
 # ---- renderer -------------------------------------------------------------------------------
-class Renderer:
-    """One render context (lux_ctx): a resident scene plus its accumulation image."""
+class ResidentScene:
+    """A scene built once on the device (lux_scene_create): geometry, BVH, materials, textures
+    and light tables. Renderers made on it (Renderer(resident, ...)) allocate only per-pixel
+    state, as the reference's pathtraceInit does after main() has built the scene."""
 
     def __init__(self, scene, options: Optional[Options] = None, **kw):
         self.scene = scene
         self.options = options if options is not None else default_options(**kw)
         h = C.c_void_p()
-        _check(lib().lux_init(scene.desc_ptr, C.byref(self.options), C.byref(h)))
+        _check(lib().lux_scene_create(scene.desc_ptr, C.byref(self.options), C.byref(h)))
         self._h = h
-        self.width = scene.width
-        self.height = scene.height
+
+    @property
+    def width(self) -> int:
+        return self.scene.width
+
+    @property
+    def height(self) -> int:
+        return self.scene.height
+
+    @property
+    def device_bytes(self) -> int:
+        return int(lib().lux_scene_device_bytes(self._h))
+
+    def compatible(self, opt: Options) -> bool:
+        """Whether a context with these options can render on this build."""
+        return (opt.device, opt.precision, opt.texture_storage) == (
+            self.options.device, self.options.precision, self.options.texture_storage)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().lux_scene_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Renderer:
+    """One render context (lux_ctx): a scene plus its accumulation image. `scene` is a host
+    scene (built and owned by the context, lux_init) or a ResidentScene (shared, lux_init_on_scene,
+    optionally with another camera of any resolution)."""
+
+    def __init__(self, scene, options: Optional[Options] = None, camera: Optional[CameraDesc] = None, **kw):
+        self.scene = scene
+        self.options = options if options is not None else default_options(**kw)
+        h = C.c_void_p()
+        if isinstance(scene, ResidentScene):
+            _check(lib().lux_init_on_scene(scene._h, C.byref(camera) if camera is not None else None,
+                                           C.byref(self.options), C.byref(h)))
+        else:
+            if camera is not None:
+                raise LuxError(-1, "a camera override needs a ResidentScene")
+            _check(lib().lux_init(scene.desc_ptr, C.byref(self.options), C.byref(h)))
+        self._h = h
+        self.width = camera.width if camera is not None else scene.width
+        self.height = camera.height if camera is not None else scene.height
 
     def render_iter(self, it: int, rgba8_dev: int = 0):
         _check(lib().lux_render_iter(self._h, it, C.c_void_p(rgba8_dev) if rgba8_dev else None))
@@ -436,13 +489,32 @@ class PathTracerOptions:
 
 
 _state: Optional[Renderer] = None
+_resident: Optional[ResidentScene] = None
 
 
 def pathtraceInit(scene, **kw) -> None:
-    """Allocate and upload everything for `scene` (src/pathtrace/pathtrace_buffers.cu:21-140)."""
-    global _state
+    """Allocate the per-pixel state for `scene` (src/pathtrace/pathtrace_buffers.cu:21-140).
+
+    The scene's device build (upload, BVH, light tables, textures) is made on the first call
+    for a scene object and kept, as the reference builds meshes and acceleration structures
+    once at load (src/main.cpp:199-274): a pathtraceFree(); pathtraceInit() pair on a camera
+    or option reset (src/app/render_loop.cpp:122-126) only reallocates per-pixel state.
+    sceneRelease() drops the kept build."""
+    global _state, _resident
     pathtraceFree()
-    _state = Renderer(scene, PathTracerOptions.Get().to_options(**kw))
+    opt = PathTracerOptions.Get().to_options(**kw)
+    if _resident is None or _resident.scene is not scene or not _resident.compatible(opt):
+        sceneRelease()
+        _resident = ResidentScene(scene, opt)
+    _state = Renderer(_resident, opt)
+
+
+def sceneRelease() -> None:
+    """Free the device build pathtraceInit keeps (the reference frees meshes at exit)."""
+    global _resident
+    if _resident is not None:
+        _resident.close()
+        _resident = None
 
 
 def pathtrace(pbo: int, frame: int, iteration: int) -> None:

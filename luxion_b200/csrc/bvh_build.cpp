@@ -200,7 +200,9 @@ void build_binary(const float* boxes, int n, Binary& B) {
             const int a = best_axis;
             const float lo = cb.lo[a];
             const double k = k1[a];
-            PrimRec* it = std::partition(r0, r1, [&](const PrimRec& r) { return bin_of(r.c[a], lo, k) <= best_split; });
+            // stable, so the order inside each side (which the two-primitive and coincident-centroid
+            // cases below depend on) is the input order: the device build reproduces it exactly
+            PrimRec* it = std::stable_partition(r0, r1, [&](const PrimRec& r) { return bin_of(r.c[a], lo, k) <= best_split; });
             mid = nd.begin + int(it - r0);
         } else {
             mid = nd.begin + nd.count / 2;  // coincident centroids: split the range in half
@@ -220,6 +222,14 @@ void build_binary(const float* boxes, int n, Binary& B) {
         work.push_back(l + 1);
     }
     for (int i = 0; i < n; ++i) B.order[size_t(i)] = rec[size_t(i)].id;
+}
+
+// ceil(log2(x)) for x > 0, exactly: x = m * 2^k with m in [0.5, 1) (frexp is exact), and
+// log2(x) is k - 1 when m is 0.5, else strictly between k - 1 and k.
+int ceil_log2(double x) {
+    int k = 0;
+    const double m = std::frexp(x, &k);
+    return m == 0.5 ? k - 1 : k;
 }
 
 // Quantise the child boxes of one 8-wide node. The node box is first widened by a relative
@@ -245,7 +255,7 @@ void encode_node(BVH8Node& N, const Box& nb, const Box* cbox, const bool* used) 
     for (int a = 0; a < 3; ++a) {
         double ext = hi_d[a] - double(N.p[a]);
         int e = -126;
-        if (ext > 0.0) e = int(std::ceil(std::log2(ext / 255.0)));
+        if (ext > 0.0) e = ceil_log2(ext / 255.0);
         e = std::max(-126, std::min(127, e));
         // make sure 255 steps cover the extent after the exponent rounding
         while (std::ldexp(255.0, e) < ext && e < 127) ++e;

@@ -78,10 +78,51 @@ bool invert4(const float* m, double* out) {
 
 }  // namespace
 
+// A resident scene: geometry, acceleration structure, materials, textures and light tables on
+// one device. The reference builds these once at load (mesh uploads and acceleration builds in
+// src/main.cpp:199-274, the light precompute in src/scene/scene_precompute.cpp:22-124); render
+// contexts made on it allocate only their per-pixel state. Reference counted: the creator's
+// handle and every context on the scene hold one reference each.
+struct lux_scene {
+    int device = 0;
+    DevScene S{};
+    std::vector<void*> allocs;
+    std::vector<DevTex> texs;
+    DevTex env;
+    // what the build depended on: a context must render with the same choices
+    int precision = LUX_PRECISION_PLAIN;
+    int texture_storage = LUX_TEXSTORE_FLOAT;
+    int trace_depth = 0;          // the description's RenderState::traceDepth
+    lux_camera_desc camera{};     // the description's camera
+    bool has_emissive = false;    // -dmis is possible
+    // host copies for CDF queries
+    std::vector<float> h_emissive_prefix, h_tri_prefix, h_marginal, h_conditional;
+    float h_total_area = 0.0f;
+    int64_t instanced_tris = 0;
+    size_t scene_bytes = 0;
+    std::atomic<int> refs{1};
+
+    template <class T>
+    int alloc(T** p, size_t n) {
+        int rc = dalloc(p, n);
+        if (rc == LUX_OK && *p) allocs.push_back(*p);
+        scene_bytes += n * sizeof(T);
+        return rc;
+    }
+    template <class T>
+    int up(T** p, const T* src, size_t n) {
+        int rc = upload(p, src, n);
+        if (rc == LUX_OK && *p) allocs.push_back(*p);
+        scene_bytes += n * sizeof(T);
+        return rc;
+    }
+};
+
 struct lux_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    lux_scene* scene = nullptr;   // holds one reference
     lux_options opt{};
     DevOptions dopt{};
     DevCamera cam{};
@@ -90,10 +131,8 @@ struct lux_ctx {
     int width = 0, height = 0, npix = 0;
     int spp_per_wave = 1;
     int accumulated = 0;
-    // owned device memory
+    // owned device memory (per-pixel and per-path state only)
     std::vector<void*> allocs;
-    std::vector<DevTex> texs;
-    DevTex env;
     float* image = nullptr;
     float* comp = nullptr;
     uint8_t* rgba = nullptr;
@@ -109,23 +148,11 @@ struct lux_ctx {
     bool timing = false;
     cudaEvent_t ev[2] = {nullptr, nullptr};
     std::vector<cudaEvent_t> kev;
-    // host copies for CDF queries
-    std::vector<float> h_emissive_prefix, h_tri_prefix, h_marginal, h_conditional;
-    float h_total_area = 0.0f;
-    int64_t instanced_tris = 0;
-    size_t scene_bytes = 0;
 
     template <class T>
     int alloc(T** p, size_t n) {
         int rc = dalloc(p, n);
         if (rc == LUX_OK && *p) allocs.push_back(*p);
-        return rc;
-    }
-    template <class T>
-    int up(T** p, const T* src, size_t n) {
-        int rc = upload(p, src, n);
-        if (rc == LUX_OK && *p) allocs.push_back(*p);
-        scene_bytes += n * sizeof(T);
         return rc;
     }
 };
@@ -746,17 +773,67 @@ int lux::build_host_scene(const lux_scene_desc& d, const lux_options& opt, std::
 namespace {
 
 // Host build and upload of the scene; device_work runs on the build's device thread.
-int build_scene(lux_ctx* C, const lux_scene_desc& d, const std::function<int()>& device_work) {
+int build_scene(lux_scene* R, const lux_scene_desc& d, const lux_options& opt, const std::function<int()>& device_work) {
     HostScene H;
-    int rc = build_host_scene(d, C->opt, C->texs, C->env, H, device_work);
+    int rc = build_host_scene(d, opt, R->texs, R->env, H, device_work);
     if (rc) return rc;
-    C->instanced_tris = H.instanced_tris;
-    C->h_emissive_prefix = H.emissive_prefix;
-    C->h_tri_prefix = H.tri_prefix;
-    C->h_marginal = H.marginal;
-    C->h_conditional = H.conditional;
-    C->h_total_area = H.total_area;
-    return upload_scene(C, H, C->S);
+    R->instanced_tris = H.instanced_tris;
+    R->h_emissive_prefix = H.emissive_prefix;
+    R->h_tri_prefix = H.tri_prefix;
+    R->h_marginal = H.marginal;
+    R->h_conditional = H.conditional;
+    R->h_total_area = H.total_area;
+    R->has_emissive = !H.emissive.empty() && H.total_area >= 0.00001f;
+    for (const DevTex& t : R->texs) R->scene_bytes += t.bytes;
+    R->scene_bytes += R->env.bytes;
+    return upload_scene(R, H, R->S);
+}
+
+void scene_release(lux_scene* R) {
+    if (!R || --R->refs > 0) return;
+    cudaSetDevice(R->device);
+    for (auto& t : R->texs) destroy_texture(t);
+    destroy_texture(R->env);
+    for (void* p : R->allocs) cudaFree(p);
+    delete R;
+}
+
+// Checks shared by lux_scene_create and lux_init: options, and the device (made current).
+int check_options_and_device(const lux_options& o) {
+    if (o.texture_storage < LUX_TEXSTORE_FLOAT || o.texture_storage > LUX_TEXSTORE_HALF)
+        return fail(LUX_ERR_INVALID, "unknown texture storage");
+    if (o.precision != LUX_PRECISION_PLAIN && o.precision != LUX_PRECISION_COMPENSATED)
+        return fail(LUX_ERR_INVALID, "unknown precision");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(LUX_ERR_NO_DEVICE, "no CUDA device");
+    if (o.device < 0 || o.device >= ndev) return fail(LUX_ERR_INVALID, "device ordinal out of range");
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, o.device);
+    if (prop.major < 10) return fail(LUX_ERR_NO_DEVICE, "an sm_100 device is required");
+    LUX_CUDA(cudaSetDevice(o.device));
+    return LUX_OK;
+}
+
+// Build a resident scene; device_work (may be empty) runs on the build's device thread after
+// the textures, overlapping the acceleration-structure build.
+int scene_create(const lux_scene_desc& d, const lux_options& o, const std::function<int()>& device_work,
+                 lux_scene** out) {
+    *out = nullptr;
+    lux_scene* R = new lux_scene();
+    R->device = o.device;
+    R->precision = o.precision;
+    R->texture_storage = o.texture_storage;
+    R->trace_depth = d.trace_depth;
+    R->camera = d.camera;
+    int rc = build_scene(R, d, o, device_work);
+    if (rc) {
+        std::string keep = g_err;
+        scene_release(R);
+        g_err = keep;
+        return rc;
+    }
+    *out = R;
+    return LUX_OK;
 }
 
 // The wave's arrays are carved from one allocation (each 256-byte aligned), so that a
@@ -999,34 +1076,32 @@ void lux_default_options(lux_options* o) {
 
 const char* lux_last_error(void) { return lux::g_err.c_str(); }
 
-int lux_init(const lux_scene_desc* scene, const lux_options* opt, lux_ctx** out) {
-    if (!out) return fail(LUX_ERR_INVALID, "out is NULL");
-    *out = nullptr;
-    if (!scene) return fail(LUX_ERR_INVALID, "scene is NULL");
-    const lux_scene_desc& d = *scene;
-    if (int rc = validate_scene_desc(d)) return rc;
-    lux_options o;
-    if (opt) o = *opt;
-    else lux_default_options(&o);
-    if (o.texture_storage < LUX_TEXSTORE_FLOAT || o.texture_storage > LUX_TEXSTORE_HALF)
-        return fail(LUX_ERR_INVALID, "unknown texture storage");
-    int tdepth = o.trace_depth > 0 ? o.trace_depth : d.trace_depth;
+}  // extern "C"
+
+namespace {
+
+// The context fields that follow from the options and the camera, and its stream; no device
+// memory yet. scene_depth is the scene description's trace depth.
+// Context options that need no device: trace depth and the debug views.
+int check_ctx_options(const lux_options& o, const lux_camera_desc& cd, int scene_depth) {
+    if (cd.width <= 0 || cd.height <= 0) return fail(LUX_ERR_INVALID, "camera resolution must be positive");
+    int tdepth = o.trace_depth > 0 ? o.trace_depth : scene_depth;
     if (tdepth <= 0 || tdepth > kMaxDepth) return fail(LUX_ERR_INVALID, "trace depth must be in 1..64");
     if (o.material_debug_mode < LUX_MATDEBUG_OFF || o.material_debug_mode > LUX_MATDEBUG_ALPHA)
         return fail(LUX_ERR_INVALID, "material_debug_mode must be in 0..6");
     if (o.debug_bvh != 0 && o.debug_bvh != 1) return fail(LUX_ERR_INVALID, "debug_bvh must be 0 or 1");
     if (o.debug_bvh && o.material_debug_mode)
         return fail(LUX_ERR_UNSUPPORTED, "the BVH heatmap and a material debug view are exclusive");
+    return LUX_OK;
+}
+
+int ctx_prepare(const lux_options& o, const lux_camera_desc& cd, int scene_depth, lux_ctx** out) {
+    *out = nullptr;
+    if (int rc = check_ctx_options(o, cd, scene_depth)) return rc;
+    int tdepth = o.trace_depth > 0 ? o.trace_depth : scene_depth;
     // debug views trace camera rays only (src/pathtrace.cu:107 forces trace depth 1 for the
     // material views); their camera rays are seeded with that depth as well
     if (o.material_debug_mode || o.debug_bvh) tdepth = 1;
-    int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(LUX_ERR_NO_DEVICE, "no CUDA device");
-    if (o.device < 0 || o.device >= ndev) return fail(LUX_ERR_INVALID, "device ordinal out of range");
-    cudaDeviceProp prop;
-    cudaGetDeviceProperties(&prop, o.device);
-    if (prop.major < 10) return fail(LUX_ERR_NO_DEVICE, "an sm_100 device is required");
-    LUX_CUDA(cudaSetDevice(o.device));
     lux_ctx* C = new lux_ctx();
     C->device = o.device;
     C->opt = o;
@@ -1037,10 +1112,9 @@ int lux_init(const lux_scene_desc* scene, const lux_options* opt, lux_ctx** out)
     C->dopt.color_mode = o.color_mode;
     C->dopt.precision = o.precision;
     C->dopt.material_debug = o.material_debug_mode;
-    C->width = d.camera.width;
-    C->height = d.camera.height;
+    C->width = cd.width;
+    C->height = cd.height;
     C->npix = C->width * C->height;
-    const lux_camera_desc& cd = d.camera;
     for (int a = 0; a < 3; ++a) {
         C->cam.pos[a] = cd.position[a];
         C->cam.view[a] = cd.view[a];
@@ -1051,43 +1125,148 @@ int lux_init(const lux_scene_desc* scene, const lux_options* opt, lux_ctx** out)
     C->cam.pixel_length[1] = cd.pixel_length[1];
     C->cam.width = cd.width;
     C->cam.height = cd.height;
-    auto bail = [&](int rc) {
-        std::string keep = g_err;
-        lux_free(C);
-        g_err = keep;
-        return rc;
-    };
     if (o.stream) {
         C->stream = static_cast<cudaStream_t>(o.stream);
     } else {
-        if (cudaStreamCreateWithFlags(&C->stream, cudaStreamNonBlocking) != cudaSuccess)
-            return bail(fail(LUX_ERR_CUDA, "cudaStreamCreate failed"));
+        if (cudaStreamCreateWithFlags(&C->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete C;
+            return fail(LUX_ERR_CUDA, "cudaStreamCreate failed");
+        }
         C->own_stream = true;
     }
     // samples kept in flight together: about 8M paths, at least one sample
     int spw = o.spp_per_wave > 0 ? o.spp_per_wave : std::max(1, (8 << 20) / C->npix);
     spw = std::max(1, std::min(spw, 1 << 16));
     C->spp_per_wave = spw;
-    // The wave buffers and the image do not depend on the scene: the scene build's device
-    // thread allocates them after the textures, while this thread builds the BVHs.
-    int rc = build_scene(C, d, [&]() {
-        int r = alloc_wave(C, spw * C->npix);
-        if (!r) r = C->alloc(&C->image, size_t(C->npix) * 3);
-        if (!r && o.precision == LUX_PRECISION_COMPENSATED) r = C->alloc(&C->comp, size_t(C->npix) * 3);
-        if (!r) r = C->alloc(&C->rgba, size_t(C->npix) * 4);
-        if (!r && cudaMemset(C->image, 0, size_t(C->npix) * 3 * sizeof(float)) != cudaSuccess)
-            r = fail(LUX_ERR_CUDA, "memset");
-        if (!r && C->comp && cudaMemset(C->comp, 0, size_t(C->npix) * 3 * sizeof(float)) != cudaSuccess)
-            r = fail(LUX_ERR_CUDA, "memset");
-        return r;
-    });
-    if (rc) return bail(rc);
-    cudaEventCreate(&C->ev[0]);
-    cudaEventCreate(&C->ev[1]);
+    *out = C;
+    return LUX_OK;
+}
+
+// Per-pixel and per-path device memory of a context (the part pathtraceInit allocates,
+// src/pathtrace/pathtrace_buffers.cu:21-140).
+int ctx_alloc(lux_ctx* C) {
+    int r = alloc_wave(C, C->spp_per_wave * C->npix);
+    if (!r) r = C->alloc(&C->image, size_t(C->npix) * 3);
+    if (!r && C->opt.precision == LUX_PRECISION_COMPENSATED) r = C->alloc(&C->comp, size_t(C->npix) * 3);
+    if (!r) r = C->alloc(&C->rgba, size_t(C->npix) * 4);
+    if (!r && cudaMemsetAsync(C->image, 0, size_t(C->npix) * 3 * sizeof(float), C->stream) != cudaSuccess)
+        r = fail(LUX_ERR_CUDA, "memset");
+    if (!r && C->comp && cudaMemsetAsync(C->comp, 0, size_t(C->npix) * 3 * sizeof(float), C->stream) != cudaSuccess)
+        r = fail(LUX_ERR_CUDA, "memset");
+    return r;
+}
+
+// The scene-dependent option checks of a context on R.
+int check_ctx_on_scene(const lux_scene* R, const lux_options& o) {
+    if (o.device != R->device) return fail(LUX_ERR_INVALID, "the context's device differs from the scene's");
+    if (o.precision != R->precision) return fail(LUX_ERR_INVALID, "precision differs from the scene's build");
+    if (o.texture_storage != R->texture_storage)
+        return fail(LUX_ERR_INVALID, "texture storage differs from the scene's build");
+    if (o.direct_light_sampling && !R->has_emissive)
+        return fail(LUX_ERR_INVALID, "-dmis requires the scene to contain emissive geometry");
+    if (o.env_importance_sampling && !R->S.has_env) return fail(LUX_ERR_INVALID, "-emis requires an environment map");
+    return LUX_OK;
+}
+
+int ctx_finish(lux_ctx* C) {
+    if (cudaEventCreate(&C->ev[0]) != cudaSuccess || cudaEventCreate(&C->ev[1]) != cudaSuccess)
+        return fail(LUX_ERR_CUDA, "cudaEventCreate failed");
     // occupancy queries happen here, never inside a stream capture
     for (int m = 0; m < 4; ++m) trace_grid_blocks(m);
     shade_grid_blocks();
-    if (cudaDeviceSynchronize() != cudaSuccess) return bail(fail(LUX_ERR_CUDA, cudaGetErrorString(cudaGetLastError())));
+    if (cudaStreamSynchronize(C->stream) != cudaSuccess) return fail(LUX_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
+    if (cudaGetLastError() != cudaSuccess) return fail(LUX_ERR_CUDA, "context set-up failed");
+    return LUX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lux_scene_create(const lux_scene_desc* scene, const lux_options* opt, lux_scene** out) {
+    if (!out) return fail(LUX_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!scene) return fail(LUX_ERR_INVALID, "scene is NULL");
+    if (int rc = validate_scene_desc(*scene)) return rc;
+    lux_options o;
+    if (opt) o = *opt;
+    else lux_default_options(&o);
+    if (int rc = check_options_and_device(o)) return rc;
+    // -dmis / -emis are checked per context (lux_init_on_scene), not against the scene build
+    o.direct_light_sampling = 0;
+    o.env_importance_sampling = 0;
+    int rc = scene_create(*scene, o, nullptr, out);
+    if (rc) return rc;
+    if (cudaDeviceSynchronize() != cudaSuccess) {
+        lux_scene_free(*out);
+        *out = nullptr;
+        return fail(LUX_ERR_CUDA, "scene build failed");
+    }
+    return LUX_OK;
+}
+
+int lux_scene_free(lux_scene* scene) {
+    scene_release(scene);
+    return LUX_OK;
+}
+
+int64_t lux_scene_device_bytes(const lux_scene* scene) { return scene ? int64_t(scene->scene_bytes) : 0; }
+
+int lux_init_on_scene(lux_scene* R, const lux_camera_desc* camera, const lux_options* opt, lux_ctx** out) {
+    if (!out) return fail(LUX_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!R) return fail(LUX_ERR_INVALID, "scene is NULL");
+    lux_options o;
+    if (opt) o = *opt;
+    else lux_default_options(&o);
+    if (int rc = check_ctx_options(o, camera ? *camera : R->camera, R->trace_depth)) return rc;
+    if (int rc = check_options_and_device(o)) return rc;
+    if (int rc = check_ctx_on_scene(R, o)) return rc;
+    lux_ctx* C = nullptr;
+    if (int rc = ctx_prepare(o, camera ? *camera : R->camera, R->trace_depth, &C)) return rc;
+    ++R->refs;
+    C->scene = R;
+    C->S = R->S;
+    int rc = ctx_alloc(C);
+    if (!rc) rc = ctx_finish(C);
+    if (rc) {
+        std::string keep = g_err;
+        lux_free(C);
+        g_err = keep;
+        return rc;
+    }
+    *out = C;
+    return LUX_OK;
+}
+
+int lux_init(const lux_scene_desc* scene, const lux_options* opt, lux_ctx** out) {
+    if (!out) return fail(LUX_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!scene) return fail(LUX_ERR_INVALID, "scene is NULL");
+    const lux_scene_desc& d = *scene;
+    if (int rc = validate_scene_desc(d)) return rc;
+    lux_options o;
+    if (opt) o = *opt;
+    else lux_default_options(&o);
+    if (int rc = check_ctx_options(o, d.camera, d.trace_depth)) return rc;
+    if (int rc = check_options_and_device(o)) return rc;
+    lux_ctx* C = nullptr;
+    if (int rc = ctx_prepare(o, d.camera, d.trace_depth, &C)) return rc;
+    auto bail = [&](int rc) {
+        std::string keep = g_err;
+        lux_free(C);
+        g_err = keep;
+        return rc;
+    };
+    // The wave buffers and the image do not depend on the scene: the scene build's device
+    // thread allocates them after the textures, while this thread builds the BVHs.
+    lux_scene* R = nullptr;
+    int rc = scene_create(d, o, [&]() { return ctx_alloc(C); }, &R);
+    if (rc) return bail(rc);
+    C->scene = R;  // the creation's reference passes to the context
+    C->S = R->S;
+    if ((rc = check_ctx_on_scene(R, o))) return bail(rc);
+    if ((rc = ctx_finish(C))) return bail(rc);
     *out = C;
     return LUX_OK;
 }
@@ -1173,12 +1352,6 @@ int lux_free(lux_ctx* C) {
     cudaSetDevice(C->device);
     if (C->stream) cudaStreamSynchronize(C->stream);
     for (auto& g : C->graphs) cudaGraphExecDestroy(g.second);
-    for (auto& t : C->texs) {
-        if (t.obj) cudaDestroyTextureObject(t.obj);
-        if (t.arr) cudaFreeArray(t.arr);
-    }
-    if (C->env.obj) cudaDestroyTextureObject(C->env.obj);
-    if (C->env.arr) cudaFreeArray(C->env.arr);
     for (void* p : C->allocs) cudaFree(p);
     if (C->h_wave_iter) cudaFreeHost(C->h_wave_iter);
     if (C->h_ctr) cudaFreeHost(C->h_ctr);
@@ -1186,7 +1359,9 @@ int lux_free(lux_ctx* C) {
     if (C->ev[0]) cudaEventDestroy(C->ev[0]);
     if (C->ev[1]) cudaEventDestroy(C->ev[1]);
     if (C->own_stream && C->stream) cudaStreamDestroy(C->stream);
+    lux_scene* R = C->scene;
     delete C;
+    scene_release(R);
     return LUX_OK;
 }
 
@@ -1321,10 +1496,10 @@ int lux_get_cdfs(lux_ctx* C, float* ep, float* tp, float* mg, float* cd, float* 
     if (!C) return fail(LUX_ERR_STATE, "context is NULL");
     cudaSetDevice(C->device);
     DevScene& S = C->S;
-    if (ep && S.num_emissive) LUX_CUDA(cudaMemcpy(ep, S.emissive_prefix, C->h_emissive_prefix.size() * 4, cudaMemcpyDeviceToHost));
-    if (tp && !C->h_tri_prefix.empty()) LUX_CUDA(cudaMemcpy(tp, S.tri_prefix, C->h_tri_prefix.size() * 4, cudaMemcpyDeviceToHost));
-    if (mg && S.has_env) LUX_CUDA(cudaMemcpy(mg, S.marginal, C->h_marginal.size() * 4, cudaMemcpyDeviceToHost));
-    if (cd && S.has_env) LUX_CUDA(cudaMemcpy(cd, S.conditional, C->h_conditional.size() * 4, cudaMemcpyDeviceToHost));
+    if (ep && S.num_emissive) LUX_CUDA(cudaMemcpy(ep, S.emissive_prefix, C->scene->h_emissive_prefix.size() * 4, cudaMemcpyDeviceToHost));
+    if (tp && !C->scene->h_tri_prefix.empty()) LUX_CUDA(cudaMemcpy(tp, S.tri_prefix, C->scene->h_tri_prefix.size() * 4, cudaMemcpyDeviceToHost));
+    if (mg && S.has_env) LUX_CUDA(cudaMemcpy(mg, S.marginal, C->scene->h_marginal.size() * 4, cudaMemcpyDeviceToHost));
+    if (cd && S.has_env) LUX_CUDA(cudaMemcpy(cd, S.conditional, C->scene->h_conditional.size() * 4, cudaMemcpyDeviceToHost));
     if (ta) *ta = S.total_area;
     return LUX_OK;
 }
@@ -1342,7 +1517,7 @@ int lux_rng_stream(int iter, int index, int depth, int n, float* out) {
 
 int lux_sample_texture(lux_ctx* C, int tex, const float* uv, int n, float* out) {
     if (!C || n < 0 || (n > 0 && (!uv || !out))) return fail(LUX_ERR_INVALID, "bad arguments");
-    if (tex < -1 || tex >= int(C->texs.size())) return fail(LUX_ERR_INVALID, "texture index out of range");
+    if (tex < -1 || tex >= int(C->scene->texs.size())) return fail(LUX_ERR_INVALID, "texture index out of range");
     if (tex == -1 && !C->S.has_env) return fail(LUX_ERR_INVALID, "no environment map");
     if (n == 0) return LUX_OK;
     cudaSetDevice(C->device);
@@ -1351,7 +1526,7 @@ int lux_sample_texture(lux_ctx* C, int tex, const float* uv, int n, float* out) 
     float* dout = t.get<float>(size_t(n) * 4);
     if (!du || !dout) return fail(LUX_ERR_OOM, "temporary allocation failed");
     LUX_CUDA(cudaMemcpyAsync(du, uv, size_t(n) * 2 * sizeof(float), cudaMemcpyHostToDevice, C->stream));
-    LUX_CUDA(launch_tex_ext(tex < 0 ? C->env.obj : C->texs[tex].obj, du, n, dout, C->stream));
+    LUX_CUDA(launch_tex_ext(tex < 0 ? C->scene->env.obj : C->scene->texs[tex].obj, du, n, dout, C->stream));
     LUX_CUDA(cudaMemcpyAsync(out, dout, size_t(n) * 4 * sizeof(float), cudaMemcpyDeviceToHost, C->stream));
     LUX_CUDA(cudaStreamSynchronize(C->stream));
     return LUX_OK;
