@@ -299,6 +299,16 @@ int lux_trace_rays(lux_ctx* ctx, const float* rays, int n, int mode, int iter, u
 #define LUX_TRACE_STATIC_MAX_RAYS 65536
 int lux_trace_rays_static(lux_ctx* ctx, const float* rays, int n, int mode, int iter, uint32_t* hits);
 
+/* BVH8 build parity (no counterpart in the reference; its builder is fill_bvh,
+ * src/mesh/bvh_build.cu:15-318): build the compressed 8-wide BVH over n = tree_begin[num_trees]
+ * boxes (6 floats each: min xyz, max xyz) grouped into trees [tree_begin[t], tree_begin[t+1])
+ * with the device builder (on_device = 1, the one every scene build uses) or the host builder
+ * (0, needs no device). Trees are laid out one after another; child_base is absolute, tri_base
+ * relative to the tree's first box. nodes: room for `capacity` 80-byte nodes; order: n leaf
+ * records -> box index; roots, depth: per tree; *num_nodes: nodes written. Host buffers. */
+int lux_bvh8_build(const float* boxes, const int* tree_begin, int num_trees, int on_device, void* nodes,
+                   int capacity, uint32_t* order, uint32_t* roots, int* depth, int* num_nodes);
+
 /* Morton keys of caller rays (src/morton_codes.cu:13-24, src/kernels/intersection_precompute.cu:6-33):
  * rays as in lux_trace_rays; keys: n u32. Host buffers. */
 int lux_morton_keys(lux_ctx* ctx, const float* rays, int n, uint32_t* keys);

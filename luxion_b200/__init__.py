@@ -53,6 +53,8 @@ SIGNATURES = {
     "lux_trace_rays": (C.c_int, [_P, c_float_p, C.c_int, C.c_int, C.c_int, c_u32_p]),
     "lux_trace_rays_static": (C.c_int, [_P, c_float_p, C.c_int, C.c_int, C.c_int, c_u32_p]),
     "lux_morton_keys": (C.c_int, [_P, c_float_p, C.c_int, c_u32_p]),
+    "lux_bvh8_build": (C.c_int, [c_float_p, c_int_p, C.c_int, C.c_int, C.c_void_p, C.c_int, c_u32_p, c_u32_p, c_int_p,
+                                 c_int_p]),
     "lux_shade_step": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, c_float_p, C.c_int, c_u32_p, c_int_p, c_int_p]),
     "lux_light_samples": (C.c_int, [_P, C.c_int, C.c_int, c_int_p, C.c_int, c_float_p]),
     "lux_get_cdfs": (C.c_int, [_P, c_float_p, c_float_p, c_float_p, c_float_p, c_float_p]),
@@ -185,6 +187,23 @@ def furnace(width: int = 64, height: int = 64, subdiv: int = 16, vertex_normals:
         else:
             setattr(m, k, v)
     return HostScene(lib().lux_scene_furnace_material(width, height, subdiv, C.byref(m), 1 if vertex_normals else 0))
+
+
+def bvh8_build(boxes: np.ndarray, tree_begin, on_device: bool):
+    """Build the 8-wide BVH over boxes (n x 6: min, max) grouped into trees (lux_bvh8_build).
+    Returns (nodes as an n_nodes x 80 uint8 array, leaf order, roots, depths)."""
+    boxes = np.ascontiguousarray(boxes, np.float32)
+    tb = np.ascontiguousarray(tree_begin, np.int32)
+    n, g = int(tb[-1]), len(tb) - 1
+    cap = max(2 * n, 16)
+    nodes = np.zeros((cap, 80), np.uint8)
+    order = np.zeros(n, np.uint32)
+    roots = np.zeros(g, np.uint32)
+    depth = np.zeros(g, np.int32)
+    nn = C.c_int(0)
+    _check(lib().lux_bvh8_build(ptr(boxes), ptr(tb, C.c_int), g, 1 if on_device else 0, nodes.ctypes.data, cap,
+                                ptr(order, C.c_uint32), ptr(roots, C.c_uint32), ptr(depth, C.c_int), C.byref(nn)))
+    return nodes[: nn.value], order, roots, depth
 
 
 # ---- renderer -------------------------------------------------------------------------------

@@ -10,7 +10,9 @@ Translation units:
   sort.cu     Morton keys and the radix sort of a bounce queue
   trace_static.cu  the fixed device scratch of lux_trace_rays_static
   texconv.cu  texel conversion (8/16-bit to float or binary16) at scene upload
-  context.cpp, engine.cpp, bvh_build.cpp, scene_gen.cpp   host C++ (no FMA contraction)
+  bvh_gpu.cu  device BVH8 build (binned SAH + collapse) and scene-geometry kernels,
+              --fmad=false so every step rounds as the host builder's does
+  context.cpp, engine.cpp, geometry.cpp, bvh_build.cpp, scene_gen.cpp   host C++ (no FMA contraction)
 The CUDA runtime is linked statically so the library does not depend on which libcudart a
 host process (for example PyTorch) has already loaded.
 """
@@ -37,9 +39,10 @@ CU_UNITS = {
     "shade.cu": ["--fmad=false"],
     "sort.cu": ["--fmad=true"],
     "trace_static.cu": ["--fmad=true"],
+    "bvh_gpu.cu": ["--fmad=false"],
     "texconv.cu": ["--fmad=false"],
 }
-CPP_UNITS = ["context.cpp", "engine.cpp", "bvh_build.cpp", "scene_gen.cpp"]
+CPP_UNITS = ["context.cpp", "engine.cpp", "geometry.cpp", "bvh_build.cpp", "scene_gen.cpp"]
 
 
 def _sources():

@@ -48,35 +48,6 @@ int fail(int code, const std::string& msg) {
 
 }  // namespace lux
 
-namespace {
-
-bool invert4(const float* m, double* out) {
-    double t[4][8];
-    for (int r = 0; r < 4; ++r)
-        for (int c = 0; c < 4; ++c) {
-            t[r][c] = m[c * 4 + r];
-            t[r][c + 4] = (r == c) ? 1.0 : 0.0;
-        }
-    for (int c = 0; c < 4; ++c) {
-        int p = c;
-        for (int r = c + 1; r < 4; ++r)
-            if (std::fabs(t[r][c]) > std::fabs(t[p][c])) p = r;
-        if (std::fabs(t[p][c]) < 1e-300) return false;
-        for (int k = 0; k < 8; ++k) std::swap(t[c][k], t[p][k]);
-        double d = t[c][c];
-        for (int k = 0; k < 8; ++k) t[c][k] /= d;
-        for (int r = 0; r < 4; ++r)
-            if (r != c) {
-                double f = t[r][c];
-                for (int k = 0; k < 8; ++k) t[r][k] -= f * t[c][k];
-            }
-    }
-    for (int r = 0; r < 4; ++r)
-        for (int c = 0; c < 4; ++c) out[c * 4 + r] = t[r][c + 4];
-    return true;
-}
-
-}  // namespace
 
 // A resident scene: geometry, acceleration structure, materials, textures and light tables on
 // one device. The reference builds these once at load (mesh uploads and acceleration builds in
@@ -413,9 +384,7 @@ int pow2_at_least(int v) {
 
 int lux::build_host_scene(const lux_scene_desc& d, const lux_options& opt, std::vector<DevTex>& texs,
                           DevTex& env, HostScene& H, const std::function<int()>& device_work) {
-    const int NM = d.num_meshes;
-    const int NI = d.num_instances;
-    // ---- textures and the environment map, on their own thread during the BLAS builds ----
+    // ---- textures and the environment map, on their own thread during the light tables ----
     const size_t tex0 = texs.size();
     texs.resize(tex0 + d.num_textures);
     int dev = 0;
@@ -448,230 +417,42 @@ int lux::build_host_scene(const lux_scene_desc& d, const lux_options& opt, std::
         }
     } joiner{texer};
 
-    // ---- per-mesh BLAS, triangle records and vertex data (threaded across meshes) ----
-    // Triangle, vertex and index offsets follow from the counts; node offsets only from the
-    // finished builds, so nodes are concatenated afterwards.
-    bool& any_n = H.any_n;
-    bool& any_uv = H.any_uv;
-    std::vector<size_t> tri_off(size_t(NM) + 1, 0), vert_off(size_t(NM) + 1, 0);
-    for (int m = 0; m < NM; ++m) {
-        any_n |= d.meshes[m].normals != nullptr;
-        any_uv |= d.meshes[m].uvs != nullptr;
-        tri_off[m + 1] = tri_off[m] + size_t(d.meshes[m].num_tris);
-        vert_off[m + 1] = vert_off[m] + size_t(d.meshes[m].num_verts);
+    // ---- light tables ----
+    std::vector<float> envt_tmp;
+    const float* envt = d.env_data ? env_texels(d, opt.texture_storage, envt_tmp) : nullptr;
+    std::vector<std::vector<float>> tri_prefix;
+    bool env_ok;
+    if (opt.precision == LUX_PRECISION_COMPENSATED)
+        env_ok = light_tables<double>(d, envt, H.emissive, H.emissive_prefix, tri_prefix, H.total_area, H.marginal,
+                                      H.conditional);
+    else
+        env_ok = light_tables<float>(d, envt, H.emissive, H.emissive_prefix, tri_prefix, H.total_area, H.marginal,
+                                     H.conditional);
+    if (!env_ok) return fail(LUX_ERR_INVALID, "environment map has no emission");
+    if (d.env_data) {
+        // about one marginal entry and four conditional entries per guide cell
+        const int W = d.env_width, Hh = d.env_height;
+        H.guide_marg = pow2_at_least(Hh);
+        H.guide_cond = pow2_at_least(std::max(1, W / 4));
+        H.marginal_guide.resize(size_t(H.guide_marg) + 1);
+        cdf_guide(H.marginal.data(), Hh, H.guide_marg, H.marginal_guide.data());
+        H.conditional_guide.resize(size_t(H.guide_cond + 1) * Hh);
+        parallel_chunks(Hh, [&](int y0, int y1) {
+            for (int y = y0; y < y1; ++y)
+                cdf_guide(H.conditional.data() + size_t(y) * W, W, H.guide_cond,
+                          H.conditional_guide.data() + size_t(y) * (H.guide_cond + 1));
+        });
     }
-    H.prims.resize(tri_off[NM] * 3);
-    H.idx.resize(tri_off[NM] * 3);
-    H.pos.resize(vert_off[NM] * 3);
-    if (any_n) H.nrm.resize(vert_off[NM] * 3);
-    if (any_uv) H.uv.resize(vert_off[NM] * 2);
-    std::vector<BVH8Build> blas(NM);
-    std::vector<float> mesh_box(size_t(NM) * 6);
-    std::atomic<bool> bad_order{false};
-    {
-        // largest meshes first, so that no large build starts last on an otherwise idle pool
-        std::vector<int> by_size(NM);
-        for (int m = 0; m < NM; ++m) by_size[m] = m;
-        std::stable_sort(by_size.begin(), by_size.end(),
-                         [&](int a, int b) { return d.meshes[a].num_tris > d.meshes[b].num_tris; });
-        std::atomic<int> next{0};
-        unsigned nt = std::max(1u, std::min(std::thread::hardware_concurrency(), 64u));
-        auto work = [&]() {
-            for (int k = next++; k < NM; k = next++) {
-                const int m = by_size[k];
-                const lux_mesh_desc& md = d.meshes[m];
-                const size_t nv = size_t(md.num_verts), ntri = size_t(md.num_tris);
-                std::vector<float> boxes(ntri * 6);
-                for (size_t k = 0; k < ntri; ++k) {
-                    float* b = &boxes[k * 6];
-                    for (int a = 0; a < 3; ++a) {
-                        b[a] = FLT_MAX;
-                        b[3 + a] = -FLT_MAX;
-                    }
-                    for (int c = 0; c < 3; ++c) {
-                        const float* v = md.positions + size_t(md.indices[k * 3 + c]) * 3;
-                        for (int a = 0; a < 3; ++a) {
-                            b[a] = std::min(b[a], v[a]);
-                            b[3 + a] = std::max(b[3 + a], v[a]);
-                        }
-                    }
-                    for (int a = 0; a < 3; ++a) {
-                        float pad = 1e-6f * std::max(std::fabs(b[a]), std::fabs(b[3 + a])) + 1e-9f;
-                        b[a] -= pad;
-                        b[3 + a] += pad;
-                    }
-                }
-                build_bvh8(boxes.data(), md.num_tris, blas[m]);
-                if (blas[m].prim_order.size() != ntri) {
-                    bad_order = true;
-                    continue;
-                }
-                // triangle records in leaf order: v0 with the triangle index in w, e1, e2
-                float4* out = H.prims.data() + tri_off[m] * 3;
-                for (uint32_t p : blas[m].prim_order) {
-                    const float* v0 = md.positions + size_t(md.indices[p * 3]) * 3;
-                    const float* v1 = md.positions + size_t(md.indices[p * 3 + 1]) * 3;
-                    const float* v2 = md.positions + size_t(md.indices[p * 3 + 2]) * 3;
-                    float pf;
-                    int32_t pi = int32_t(p);
-                    std::memcpy(&pf, &pi, 4);
-                    *out++ = make_float4(v0[0], v0[1], v0[2], pf);
-                    *out++ = make_float4(v1[0] - v0[0], v1[1] - v0[1], v1[2] - v0[2], 0.0f);
-                    *out++ = make_float4(v2[0] - v0[0], v2[1] - v0[1], v2[2] - v0[2], 0.0f);
-                }
-                std::memcpy(H.idx.data() + tri_off[m] * 3, md.indices, ntri * 3 * sizeof(uint32_t));
-                std::memcpy(H.pos.data() + vert_off[m] * 3, md.positions, nv * 3 * sizeof(float));
-                if (any_n) {
-                    float* dst = H.nrm.data() + vert_off[m] * 3;
-                    if (md.normals) std::memcpy(dst, md.normals, nv * 3 * sizeof(float));
-                    else std::fill(dst, dst + nv * 3, 0.0f);
-                }
-                if (any_uv) {
-                    float* dst = H.uv.data() + vert_off[m] * 2;
-                    if (md.uvs) std::memcpy(dst, md.uvs, nv * 2 * sizeof(float));
-                    else std::fill(dst, dst + nv * 2, 0.0f);
-                }
-                float* b = &mesh_box[size_t(m) * 6];
-                for (int a = 0; a < 3; ++a) {
-                    b[a] = FLT_MAX;
-                    b[3 + a] = -FLT_MAX;
-                }
-                for (size_t v = 0; v < nv; ++v)
-                    for (int a = 0; a < 3; ++a) {
-                        b[a] = std::min(b[a], md.positions[v * 3 + a]);
-                        b[3 + a] = std::max(b[3 + a], md.positions[v * 3 + a]);
-                    }
-            }
-        };
-        std::vector<std::thread> th;
-        for (unsigned t = 0; t + 1 < nt; ++t) th.emplace_back(work);
-        work();
-        for (auto& t : th) t.join();
+    H.tri_off.clear();
+    H.tri_prefix.clear();
+    for (int e : H.emissive) {
+        H.tri_off.push_back(int(H.tri_prefix.size()));
+        H.tri_prefix.insert(H.tri_prefix.end(), tri_prefix[e].begin(), tri_prefix[e].end());
     }
-    if (bad_order) return fail(LUX_ERR_UNSUPPORTED, "BVH leaf order does not cover every triangle once");
-    // ---- concatenate the BLAS nodes ----
-    std::vector<size_t> node_off(size_t(NM) + 1, 0);
-    int max_blas_depth = 0;
-    for (int m = 0; m < NM; ++m) {
-        node_off[m + 1] = node_off[m] + blas[m].nodes.size();
-        max_blas_depth = std::max(max_blas_depth, blas[m].depth);
-    }
-    H.nodes.reserve(node_off[NM] + size_t(NI) + 8);  // room for the TLAS nodes appended below
-    H.nodes.resize(node_off[NM]);
-    parallel_chunks(NM, [&](int m0, int m1) {
-        for (int m = m0; m < m1; ++m) {
-            BVH8Node* dst = H.nodes.data() + node_off[m];
-            const uint32_t nb = uint32_t(node_off[m]);
-            for (const BVH8Node& n : blas[m].nodes) {
-                *dst = n;
-                dst->child_base += nb;
-                ++dst;
-            }
-            std::vector<BVH8Node>().swap(blas[m].nodes);
-        }
-    });
-    std::vector<uint32_t> mesh_root(NM), mesh_prim(NM), mesh_vert(NM), mesh_idx(NM);
-    std::vector<int> mesh_flags(NM);
-    for (int m = 0; m < NM; ++m) {
-        const lux_mesh_desc& md = d.meshes[m];
-        mesh_root[m] = uint32_t(node_off[m]);
-        mesh_prim[m] = uint32_t(tri_off[m]);
-        mesh_vert[m] = uint32_t(vert_off[m]);
-        mesh_idx[m] = uint32_t(tri_off[m]);
-        mesh_flags[m] = (md.normals ? kInstHasNormals : 0) | (md.uvs ? kInstHasUVs : 0);
-    }
-    // ---- instances + TLAS ----
-    std::vector<DevInstance>& insts = H.insts;
-    insts.assign(NI, DevInstance{});
-    std::vector<float> iboxes(size_t(NI) * 6);
-    H.instanced_tris = 0;
-    for (int i = 0; i < NI; ++i) {
-        const lux_instance_desc& in = d.instances[i];
-        DevInstance& I = insts[i];
-        float inv[16], invT[16];
-        if (in.has_inverse) {
-            std::memcpy(inv, in.inverse, 64);
-            std::memcpy(invT, in.inv_transpose, 64);
-        } else {
-            double id[16];
-            if (!invert4(in.transform, id)) return fail(LUX_ERR_INVALID, "singular instance transform");
-            for (int k = 0; k < 16; ++k) inv[k] = float(id[k]);
-            for (int c = 0; c < 4; ++c)
-                for (int r = 0; r < 4; ++r) invT[c * 4 + r] = float(id[r * 4 + c]);
-        }
-        for (int c = 0; c < 4; ++c)
-            for (int r = 0; r < 3; ++r) {
-                I.M[c * 3 + r] = in.transform[c * 4 + r];
-                I.Minv[c * 3 + r] = inv[c * 4 + r];
-                I.MinvT[c * 3 + r] = invT[c * 4 + r];
-            }
-        I.mesh = in.mesh;
-        I.material = in.material;
-        I.blas_root = mesh_root[in.mesh];
-        I.prim_base = mesh_prim[in.mesh];
-        I.vert_base = mesh_vert[in.mesh];
-        I.idx_base = mesh_idx[in.mesh];
-        const lux_material_desc& mat = d.materials[in.material];
-        I.flags = mesh_flags[in.mesh] | (mat.alpha_mode != LUX_ALPHA_OPAQUE ? kInstAnyHit : 0);
-        I.num_tris = d.meshes[in.mesh].num_tris;
-        I.key = i;
-        H.instanced_tris += I.num_tris;
-    }
-    // World boxes of the instances, in double and padded. Each is the exact box of the mesh's
-    // transformed vertices: for rotated meshes it is much tighter than the box of the
-    // transformed mesh-box corners (measured on the 1M-triangle scene of 200 rotated
-    // instances: traversal per 16-spp step 67.8 against 78.6 ms, BVH8 node visits plus
-    // triangle tests per camera ray 16.6 against 20.5). Above 64M vertex transforms in total
-    // (heavily instanced scenes) every instance takes the corner box instead.
-    size_t vertex_work = 0;
-    for (int i = 0; i < NI; ++i) vertex_work += size_t(d.meshes[d.instances[i].mesh].num_verts);
-    const bool exact_boxes = vertex_work <= (size_t(64) << 20);
-    parallel_chunks(NI, [&](int i0, int i1) {
-        for (int i = i0; i < i1; ++i) {
-            const lux_instance_desc& in = d.instances[i];
-            const lux_mesh_desc& md = d.meshes[in.mesh];
-            double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-            auto grow = [&](double x, double y, double z) {
-                for (int a = 0; a < 3; ++a) {
-                    double w = double(in.transform[0 * 4 + a]) * x + double(in.transform[1 * 4 + a]) * y +
-                               double(in.transform[2 * 4 + a]) * z + double(in.transform[3 * 4 + a]);
-                    lo[a] = std::min(lo[a], w);
-                    hi[a] = std::max(hi[a], w);
-                }
-            };
-            if (exact_boxes) {
-                for (int v = 0; v < md.num_verts; ++v) {
-                    const float* p = md.positions + size_t(v) * 3;
-                    grow(p[0], p[1], p[2]);
-                }
-            } else {
-                const float* mb = &mesh_box[size_t(in.mesh) * 6];
-                for (int c = 0; c < 8; ++c) grow((c & 1) ? mb[3] : mb[0], (c & 2) ? mb[4] : mb[1], (c & 4) ? mb[5] : mb[2]);
-            }
-            double mext = 0, mabs = 0;
-            for (int a = 0; a < 3; ++a) {
-                mext = std::max(mext, hi[a] - lo[a]);
-                mabs = std::max(mabs, std::max(std::fabs(lo[a]), std::fabs(hi[a])));
-            }
-            double pad = 1e-5 * mext + 1e-6 * mabs + 1e-12;
-            float* b = &iboxes[size_t(i) * 6];
-            for (int a = 0; a < 3; ++a) {
-                b[a] = float(lo[a] - pad);
-                b[3 + a] = float(hi[a] + pad);
-            }
-        }
-    });
-    BVH8Build tl;
-    build_bvh8(iboxes.data(), NI, tl);
-    uint32_t tlas_root = uint32_t(H.nodes.size());
-    H.tlas_root = tlas_root;
-    for (BVH8Node n : tl.nodes) {
-        n.child_base += tlas_root;
-        H.nodes.push_back(n);
-    }
-    H.tlas_prims.assign(tl.prim_order.begin(), tl.prim_order.end());
-    if (tl.depth + max_blas_depth + 4 > 16 + 48)
-        return fail(LUX_ERR_UNSUPPORTED, "acceleration structure deeper than the traversal stack");
+    if (opt.direct_light_sampling && (H.emissive.empty() || H.total_area < 0.00001f))
+        return fail(LUX_ERR_INVALID, "-dmis requires the scene to contain emissive geometry");
+    if (opt.env_importance_sampling && !d.env_data)
+        return fail(LUX_ERR_INVALID, "-emis requires an environment map");
     // ---- materials + textures ----
     texer.join();
     if (tex_rc) return fail(tex_rc, tex_err);
@@ -716,42 +497,6 @@ int lux::build_host_scene(const lux_scene_desc& d, const lux_options& opt, std::
         tt(s.normal_tt, m.normal_tt);
         tt(s.metallic_roughness_tt, m.mr_tt);
     }
-    // ---- light tables ----
-    std::vector<float> envt_tmp;
-    const float* envt = d.env_data ? env_texels(d, opt.texture_storage, envt_tmp) : nullptr;
-    std::vector<std::vector<float>> tri_prefix;
-    bool env_ok;
-    if (opt.precision == LUX_PRECISION_COMPENSATED)
-        env_ok = light_tables<double>(d, envt, H.emissive, H.emissive_prefix, tri_prefix, H.total_area, H.marginal,
-                                      H.conditional);
-    else
-        env_ok = light_tables<float>(d, envt, H.emissive, H.emissive_prefix, tri_prefix, H.total_area, H.marginal,
-                                     H.conditional);
-    if (!env_ok) return fail(LUX_ERR_INVALID, "environment map has no emission");
-    if (d.env_data) {
-        // about one marginal entry and four conditional entries per guide cell
-        const int W = d.env_width, Hh = d.env_height;
-        H.guide_marg = pow2_at_least(Hh);
-        H.guide_cond = pow2_at_least(std::max(1, W / 4));
-        H.marginal_guide.resize(size_t(H.guide_marg) + 1);
-        cdf_guide(H.marginal.data(), Hh, H.guide_marg, H.marginal_guide.data());
-        H.conditional_guide.resize(size_t(H.guide_cond + 1) * Hh);
-        parallel_chunks(Hh, [&](int y0, int y1) {
-            for (int y = y0; y < y1; ++y)
-                cdf_guide(H.conditional.data() + size_t(y) * W, W, H.guide_cond,
-                          H.conditional_guide.data() + size_t(y) * (H.guide_cond + 1));
-        });
-    }
-    H.tri_off.clear();
-    H.tri_prefix.clear();
-    for (int e : H.emissive) {
-        H.tri_off.push_back(int(H.tri_prefix.size()));
-        H.tri_prefix.insert(H.tri_prefix.end(), tri_prefix[e].begin(), tri_prefix[e].end());
-    }
-    if (opt.direct_light_sampling && (H.emissive.empty() || H.total_area < 0.00001f))
-        return fail(LUX_ERR_INVALID, "-dmis requires the scene to contain emissive geometry");
-    if (opt.env_importance_sampling && !d.env_data)
-        return fail(LUX_ERR_INVALID, "-emis requires an environment map");
     if (d.env_data) {
         H.env_w = d.env_width;
         H.env_h = d.env_height;
@@ -760,11 +505,17 @@ int lux::build_host_scene(const lux_scene_desc& d, const lux_options& opt, std::
     }
     // Morton box: the first instance's mesh bounds padded by 1e-5 (EPSILON of
     // include/utilities.h:16), in that instance's object space
-    if (NI > 0) {
-        const float* mb = &mesh_box[size_t(d.instances[0].mesh) * 6];
+    if (d.num_instances > 0) {
+        const lux_mesh_desc& m0 = d.meshes[d.instances[0].mesh];
+        float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+        for (int v = 0; v < m0.num_verts; ++v)
+            for (int a = 0; a < 3; ++a) {
+                lo[a] = std::min(lo[a], m0.positions[size_t(v) * 3 + a]);
+                hi[a] = std::max(hi[a], m0.positions[size_t(v) * 3 + a]);
+            }
         for (int a = 0; a < 3; ++a) {
-            H.morton_bmin[a] = mb[a] - 0.00001f;
-            H.morton_bmax[a] = mb[3 + a] + 0.00001f;
+            H.morton_bmin[a] = lo[a] - 0.00001f;
+            H.morton_bmax[a] = hi[a] + 0.00001f;
         }
     }
     return LUX_OK;
@@ -774,10 +525,33 @@ namespace {
 
 // Host build and upload of the scene; device_work runs on the build's device thread.
 int build_scene(lux_scene* R, const lux_scene_desc& d, const lux_options& opt, const std::function<int()>& device_work) {
+    // The device geometry (vertex uploads, every BVH) is built on its own thread and stream,
+    // while this thread builds the light tables and the texture thread uploads the textures.
+    const int dev = R->device;
+    GeometryBuild G;
+    DevScene geo{};
+    int geo_rc = LUX_OK;
+    std::string geo_err;
+    std::thread geom([&]() {
+        cudaStream_t st = nullptr;
+        if (cudaSetDevice(dev) != cudaSuccess || cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+            geo_rc = fail(LUX_ERR_CUDA, "geometry thread set-up failed");
+            geo_err = g_err;
+            return;
+        }
+        const lux_scene_desc* one = &d;
+        geo_rc = build_geometry(&one, 1, std::vector<int>{0},
+                                [&](void** p, size_t bytes) { return R->alloc(reinterpret_cast<char**>(p), bytes); },
+                                st, geo, G);
+        if (geo_rc) geo_err = g_err;
+        cudaStreamDestroy(st);
+    });
     HostScene H;
     int rc = build_host_scene(d, opt, R->texs, R->env, H, device_work);
+    geom.join();
     if (rc) return rc;
-    R->instanced_tris = H.instanced_tris;
+    if (geo_rc) return fail(geo_rc, geo_err);
+    R->instanced_tris = G.instanced_tris[0];
     R->h_emissive_prefix = H.emissive_prefix;
     R->h_tri_prefix = H.tri_prefix;
     R->h_marginal = H.marginal;
@@ -786,7 +560,9 @@ int build_scene(lux_scene* R, const lux_scene_desc& d, const lux_options& opt, c
     R->has_emissive = !H.emissive.empty() && H.total_area >= 0.00001f;
     for (const DevTex& t : R->texs) R->scene_bytes += t.bytes;
     R->scene_bytes += R->env.bytes;
-    return upload_scene(R, H, R->S);
+    R->S = geo;
+    if ((rc = upload_scene_materials(R, H, R->S))) return rc;
+    return upload_scene_lights(R, H, R->S);
 }
 
 void scene_release(lux_scene* R) {

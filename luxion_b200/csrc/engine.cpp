@@ -106,51 +106,17 @@ struct lux_engine {
         scene_bytes += int64_t(n * sizeof(T));
         return rc;
     }
+    // device allocation counted as scene memory (the device-built geometry)
+    int up_alloc(char** p, size_t n) {
+        int rc = dalloc(p, n);
+        if (rc == LUX_OK && *p) allocs.push_back(*p);
+        scene_bytes += int64_t(n);
+        return rc;
+    }
     int64_t device_bytes() const { return scene_bytes + wave_bytes + job_bytes; }
 };
 
 namespace {
-
-// Append scene H to the concatenation A, offsetting every cross-reference. Returns the
-// scene's TLAS root in A.
-uint32_t append_scene(HostScene& A, const HostScene& H) {
-    const uint32_t no = uint32_t(A.nodes.size());
-    const uint32_t np = uint32_t(A.prims.size() / 3);
-    const uint32_t ni = uint32_t(A.insts.size());
-    const uint32_t ntp = uint32_t(A.tlas_prims.size());
-    const uint32_t nv = uint32_t(A.pos.size() / 3);
-    const uint32_t nidx = uint32_t(A.idx.size() / 3);
-    const int nm = int(A.mats.size());
-    for (size_t k = 0; k < H.nodes.size(); ++k) {
-        BVH8Node n = H.nodes[k];
-        n.child_base += no;
-        if (k >= H.tlas_root) n.tri_base += ntp;  // TLAS leaves index the TLAS-leaf array
-        A.nodes.push_back(n);
-    }
-    A.prims.insert(A.prims.end(), H.prims.begin(), H.prims.end());
-    for (DevInstance I : H.insts) {
-        I.blas_root += no;
-        I.prim_base += np;
-        I.vert_base += nv;
-        I.idx_base += nidx;
-        I.material += nm;
-        A.insts.push_back(I);
-    }
-    for (uint32_t v : H.tlas_prims) A.tlas_prims.push_back(v + ni);
-    A.pos.insert(A.pos.end(), H.pos.begin(), H.pos.end());
-    if (A.any_n) {
-        if (H.any_n) A.nrm.insert(A.nrm.end(), H.nrm.begin(), H.nrm.end());
-        else A.nrm.insert(A.nrm.end(), H.pos.size(), 0.0f);
-    }
-    if (A.any_uv) {
-        if (H.any_uv) A.uv.insert(A.uv.end(), H.uv.begin(), H.uv.end());
-        else A.uv.insert(A.uv.end(), H.pos.size() / 3 * 2, 0.0f);
-    }
-    A.idx.insert(A.idx.end(), H.idx.begin(), H.idx.end());
-    A.mats.insert(A.mats.end(), H.mats.begin(), H.mats.end());
-    A.instanced_tris += H.instanced_tris;
-    return H.tlas_root + no;
-}
 
 // Admitted jobs with samples still to schedule, in the order they fill a wave.
 int order_jobs(const lux_engine* E, std::vector<int>& order) {
@@ -314,22 +280,30 @@ int lux_engine_create(const lux_scene_desc* const* scenes, int num_scenes, const
     if (cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking) != cudaSuccess)
         return bail(fail(LUX_ERR_CUDA, "cudaStreamCreate failed"));
 
-    // ---- scenes: build each, concatenate, upload once ----
-    HostScene all;
+    // ---- scenes: geometry of all scenes built on the device at once, then each scene's
+    // textures, materials and light tables ----
     std::vector<HostScene> hs(num_scenes);
+    std::vector<int> mat_base(num_scenes, 0);
+    for (int i = 1; i < num_scenes; ++i) mat_base[i] = mat_base[i - 1] + scenes[i - 1]->num_materials;
+    GeometryBuild G;
+    if (int rc = build_geometry(scenes, num_scenes, mat_base,
+                                [&](void** p, size_t bytes) { return E->up_alloc(reinterpret_cast<char**>(p), bytes); },
+                                E->stream, E->S, G))
+        return bail(rc);
     E->envs.resize(num_scenes);
+    std::vector<DevMaterial> mats;
     for (int i = 0; i < num_scenes; ++i) {
         if (int rc = build_host_scene(*scenes[i], o, E->texs, E->envs[i], hs[i])) return bail(rc);
-        all.any_n |= hs[i].any_n;
-        all.any_uv |= hs[i].any_uv;
         E->scene_depth.push_back(scenes[i]->trace_depth);
+        E->scene_root.push_back(G.tlas_root[i]);
+        for (int& e : hs[i].emissive) e += G.inst_base[i];  // emissive instances in the concatenation
+        mats.insert(mats.end(), hs[i].mats.begin(), hs[i].mats.end());
     }
-    for (int i = 0; i < num_scenes; ++i) {
-        const uint32_t ni = uint32_t(all.insts.size());
-        E->scene_root.push_back(append_scene(all, hs[i]));
-        for (int& e : hs[i].emissive) e += int(ni);  // emissive instances in the concatenation
+    {
+        DevMaterial* dm = nullptr;
+        if (int rc = E->up(&dm, mats.data(), mats.size())) return bail(rc);
+        E->S.mats = dm;
     }
-    if (int rc = upload_scene(E, all, E->S)) return bail(rc);
     std::vector<DevScene> views(num_scenes);
     for (int i = 0; i < num_scenes; ++i) {
         DevScene& v = views[i];

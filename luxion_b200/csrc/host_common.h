@@ -11,6 +11,7 @@
 
 #include <cstdint>
 #include <cstring>
+#include <algorithm>
 #include <functional>
 #include <string>
 #include <vector>
@@ -57,9 +58,6 @@ inline void destroy_texture(DevTex& t) {
     t = DevTex{};
 }
 
-// Everything a resident scene needs, built on the host (textures are created on the device
-// here because materials hold their texture objects): per-mesh BLASes concatenated, the
-// TLAS appended after them, instances, materials and the light tables.
 // Allocator whose value-less construct leaves trivially constructible elements uninitialised:
 // the large host arrays of a scene are sized once and first written (and paged in) by the
 // threads that fill them, not zero-filled by one thread beforehand.
@@ -84,17 +82,12 @@ struct NoInitAlloc : std::allocator<T> {
 template <class T>
 using HostVec = std::vector<T, NoInitAlloc<T>>;
 
+// The host-built part of a resident scene: materials (textures are created on the device here
+// because materials hold their texture objects) and the light tables. The geometry (vertex
+// data, BVHs, triangle and instance records) is built on the device by build_geometry.
 struct HostScene {
-    HostVec<BVH8Node> nodes;
-    uint32_t tlas_root = 0;           // first TLAS node; nodes from here on are the TLAS
-    HostVec<float4> prims;
-    std::vector<DevInstance> insts;
-    std::vector<uint32_t> tlas_prims;
-    HostVec<float> pos, nrm, uv;
-    HostVec<uint32_t> idx;
-    bool any_n = false, any_uv = false;
     std::vector<DevMaterial> mats;
-    std::vector<int> emissive;        // emissive instances
+    std::vector<int> emissive;        // emissive instances (scene-local)
     std::vector<float> emissive_prefix, tri_prefix, marginal, conditional;
     std::vector<int> marginal_guide, conditional_guide;  // guide tables of the HDRI CDFs
     int guide_marg = 0, guide_cond = 0;
@@ -104,17 +97,38 @@ struct HostScene {
     unsigned long long env_tex = 0;
     bool has_env = false;
     float morton_bmin[3] = {0, 0, 0}, morton_bmax[3] = {0, 0, 0};
-    int64_t instanced_tris = 0;
 };
+
+// Device allocation that the owner records (and frees with everything else it owns).
+using DevAlloc = std::function<int(void** p, size_t bytes)>;
+
+// What build_geometry reports besides the DevScene geometry fields.
+struct GeometryBuild {
+    std::vector<uint32_t> tlas_root;      // per scene
+    std::vector<int64_t> instanced_tris;  // per scene
+    std::vector<int> inst_base;           // per scene (+ total): first instance in the concatenation
+    std::vector<int> max_blas_depth;      // per scene
+    uint32_t blas_nodes = 0, tlas_nodes = 0;
+    size_t bytes = 0;                     // device bytes allocated through alloc
+};
+
+// Device geometry of ns scenes concatenated (geometry.cpp): vertex data, every mesh's BLAS and
+// every scene's TLAS built on the device, triangle records, instance records (materials
+// offset by material_base[s]) and TLAS leaf records. Fills S.nodes, prims, insts, tlas_prims,
+// tlas_leaf, tlas_root (scene 0), num_insts, pos, nrm, uv, idx. Runs on stream st and returns
+// once the build has finished.
+int build_geometry(const lux_scene_desc* const* scenes, int ns, const std::vector<int>& material_base,
+                   const DevAlloc& alloc, cudaStream_t st, DevScene& S, GeometryBuild& G);
 
 // Check a scene description (sizes, index ranges, references, environment format).
 int validate_scene_desc(const lux_scene_desc& d);
 
-// Build of one validated scene description with the given options (texture storage,
-// precision, which light tables -dmis / -emis require). Textures are appended to texs; the
-// environment map goes to env. Textures are created on a second thread while the BVHs are
-// built; device_work, when given, runs on that thread after them and its status is returned
-// like a texture failure. The thread is joined before the function returns.
+// Host-side build of one validated scene description with the given options (texture
+// storage, precision, which light tables -dmis / -emis require): textures, materials, light
+// tables and the Morton box. Textures are appended to texs and created on a second thread;
+// the environment map goes to env. device_work, when given, runs on that thread after the
+// textures and its status is returned like a texture failure. The thread is joined before the
+// function returns.
 int build_host_scene(const lux_scene_desc& d, const lux_options& opt, std::vector<DevTex>& texs, DevTex& env,
                      HostScene& H, const std::function<int()>& device_work = nullptr);
 
@@ -159,57 +173,13 @@ int upload_scene_lights(Owner* C, const HostScene& H, DevScene& S) {
     return LUX_OK;
 }
 
-// Upload a host scene (geometry, materials, then its light tables). Empty arrays upload as
-// null pointers.
+// Upload the materials of a host scene.
 template <class Owner>
-int upload_scene(Owner* C, const HostScene& H, DevScene& S) {
-    std::memset(&S, 0, sizeof(S));
-    int rc;
-    uint4* dn = nullptr;
-    if ((rc = C->up(&dn, reinterpret_cast<const uint4*>(H.nodes.data()), H.nodes.size() * 5))) return rc;
-    S.nodes = dn;
-    float4* dp = nullptr;
-    if ((rc = C->up(&dp, H.prims.data(), H.prims.size()))) return rc;
-    S.prims = dp;
-    DevInstance* di = nullptr;
-    if ((rc = C->up(&di, H.insts.data(), H.insts.size()))) return rc;
-    S.insts = di;
-    uint32_t* dt = nullptr;
-    if ((rc = C->up(&dt, H.tlas_prims.data(), H.tlas_prims.size()))) return rc;
-    S.tlas_prims = dt;
-    std::vector<float4> leaf(H.tlas_prims.size() * 4);
-    for (size_t k = 0; k < H.tlas_prims.size(); ++k) {
-        const DevInstance& I = H.insts[H.tlas_prims[k]];
-        float4* q = &leaf[k * 4];
-        q[0] = make_float4(I.Minv[0], I.Minv[1], I.Minv[2], I.Minv[3]);
-        q[1] = make_float4(I.Minv[4], I.Minv[5], I.Minv[6], I.Minv[7]);
-        q[2] = make_float4(I.Minv[8], I.Minv[9], I.Minv[10], I.Minv[11]);
-        const uint32_t e[4] = {I.blas_root, I.prim_base, uint32_t(I.flags), H.tlas_prims[k]};
-        std::memcpy(&q[3], e, 16);
-    }
-    float4* dl = nullptr;
-    if ((rc = C->up(&dl, leaf.data(), leaf.size()))) return rc;
-    S.tlas_leaf = dl;
-    S.tlas_root = H.tlas_root;
-    S.num_insts = int(H.insts.size());
-    float* f = nullptr;
-    if ((rc = C->up(&f, H.pos.data(), H.pos.size()))) return rc;
-    S.pos = f;
-    if (H.any_n) {
-        if ((rc = C->up(&f, H.nrm.data(), H.nrm.size()))) return rc;
-        S.nrm = f;
-    }
-    if (H.any_uv) {
-        if ((rc = C->up(&f, H.uv.data(), H.uv.size()))) return rc;
-        S.uv = f;
-    }
-    uint32_t* du = nullptr;
-    if ((rc = C->up(&du, H.idx.data(), H.idx.size()))) return rc;
-    S.idx = du;
+int upload_scene_materials(Owner* C, const HostScene& H, DevScene& S) {
     DevMaterial* dm = nullptr;
-    if ((rc = C->up(&dm, H.mats.data(), H.mats.size()))) return rc;
+    if (int rc = C->up(&dm, H.mats.data(), H.mats.size())) return rc;
     S.mats = dm;
-    return upload_scene_lights(C, H, S);
+    return LUX_OK;
 }
 
 }  // namespace lux
