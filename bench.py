@@ -470,6 +470,7 @@ def main():
     ap.add_argument("--no-forms", action="store_true")
     ap.add_argument("--forms-only", action="store_true", help="run only the batched and served forms")
     ap.add_argument("--serve-requests", type=int, default=256)
+    ap.add_argument("--fp64-crop", type=int, default=32, help="side of the FP64-integrator crop (precision form)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -480,7 +481,7 @@ def main():
         run_reference_arm(args, rank, world)
         return
     if args.forms_only:
-        print(json.dumps({"precision": run_precision(), "batched": run_batched(),
+        print(json.dumps({"precision": run_precision(crop=args.fp64_crop), "batched": run_batched(),
                           "served": run_served(requests=args.serve_requests)}), flush=True)
         return
 
@@ -639,7 +640,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_forms:
         batched = run_batched()
         served = run_served(requests=args.serve_requests)
-        precision = run_precision()
+        precision = run_precision(crop=args.fp64_crop)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
