@@ -28,7 +28,7 @@ from typing import List, Optional
 
 import numpy as np
 
-from . import _ffi
+from . import _ffi, glmf
 from .scene_builder import SceneBuilder, default_material
 
 _COMPONENT = {5120: np.int8, 5121: np.uint8, 5122: np.int16, 5123: np.uint16, 5125: np.uint32, 5126: np.float32}
@@ -121,26 +121,29 @@ class _Model:
         return np.asarray(img.convert("RGBA"), np.uint8)
 
 
-def _quat_mat(x, y, z, w) -> np.ndarray:
-    """glm::mat4_cast of the unit quaternion (w, x, y, z)."""
-    return np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y), 0],
-                     [2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x), 0],
-                     [2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y), 0],
-                     [0, 0, 0, 1]], np.float64)
+def _libm():
+    import ctypes
+    import ctypes.util
+    lm = ctypes.CDLL(ctypes.util.find_library("m") or "libm.so.6")
+    for fn in (lm.tanf, lm.atanf):
+        fn.restype, fn.argtypes = ctypes.c_float, [ctypes.c_float]
+    return lm
 
 
 def _node_matrix(node) -> np.ndarray:
+    """The node's local matrix as the reference composes it in float (glm column-major):
+    the matrix if given, else translate(I, t) * mat4_cast(q) then scale(., s)
+    (src/scene/scene_load_gltf.cpp:250-290)."""
     if "matrix" in node:
-        return np.asarray(node["matrix"], np.float64).reshape(4, 4).T  # column-major in the file
-    M = np.eye(4)
+        return np.asarray(node["matrix"], np.float64).reshape(4, 4).astype(np.float32)  # columns in the file
+    M = glmf.identity()
     if "translation" in node:
-        T = np.eye(4)
-        T[:3, 3] = node["translation"]
-        M = M @ T
+        M = glmf.translate(M, node["translation"])
     if "rotation" in node:
-        M = M @ _quat_mat(*node["rotation"])
+        x, y, z, w = node["rotation"]
+        M = glmf.mul(M, glmf.mat4_cast(w, x, y, z))
     if "scale" in node:
-        M = M @ np.diag(list(node["scale"]) + [1.0])
+        M = glmf.scale(M, node["scale"])
     return M
 
 
@@ -184,7 +187,7 @@ def load(path: str) -> SceneBuilder:
         return int(info["index"])
 
     # materials: 0 = the reference's default (red), then the file's
-    red = default_material(color=(1.0, 0.0, 0.0), roughness=0.0, metallic=0.0, ior=0.0)
+    red = default_material(color=(1.0, 0.0, 0.0), roughness=0.0, metallic=0.0, ior=0.0, emission_strength=0.0)
     sb.add_material(red)
     for m in doc.get("materials", []):
         pbr = m.get("pbrMetallicRoughness", {})
@@ -241,14 +244,16 @@ def load(path: str) -> SceneBuilder:
 
     def visit(ni: int, parent: np.ndarray):
         node = nodes[ni]
-        G = parent @ _node_matrix(node)
+        G = glmf.mul(parent, _node_matrix(node))  # global = parent * local, in float
         if "mesh" in node:
+            inv, inv_t = glmf.inverse(G), glmf.inverse_transpose(G)
             for pi in range(len(doc["meshes"][node["mesh"]]["primitives"])):
                 pm = prim_mesh(node["mesh"], pi)
                 if pm is None:
                     continue
                 mesh, mat = pm
-                sb.add_instance(mesh, mat + 1 if mat >= 0 else 0, G)
+                # row-major for the builder; inverse and inverse transpose as glm computes them
+                sb.add_instance(mesh, mat + 1 if mat >= 0 else 0, G.T, inverse=inv.T, inv_transpose=inv_t.T)
         if "camera" in node:
             if camera:
                 raise GltfError("more than one camera in the scene")
@@ -260,7 +265,7 @@ def load(path: str) -> SceneBuilder:
     si = doc.get("scene", 0)
     roots = scenes[si]["nodes"] if scenes else list(range(len(nodes)))
     for r in roots:
-        visit(r, np.eye(4))
+        visit(r, glmf.identity())
     if not sb.instances:
         raise GltfError("no triangle meshes in the scene")
     if not camera:
@@ -274,23 +279,26 @@ def load(path: str) -> SceneBuilder:
     else:
         w = 1000
         h = int(np.float32(w) / np.float32(aspect))
-    fovy = float(np.float32(math.degrees(persp.get("yfov", math.radians(45.0)))))
-    Gf = G.astype(np.float32)
+    # glm::degrees of the double yfov, stored as float
+    fovy = float(np.float32(persp.get("yfov", math.radians(45.0)) * 57.295779513082320876798154814105))
     cam = _ffi.CameraDesc()
     cam.width, cam.height = w, h
-    eye = Gf[:3, 3]
-    view = -_normalize_f32(Gf[:3, 2][None])[0]
-    right = _normalize_f32(Gf[:3, 0][None])[0]
-    up = _normalize_f32(Gf[:3, 1][None])[0]
+    eye = G[3][:3]
+    view = -glmf.normalize(G[2][:3])
+    right = glmf.normalize(G[0][:3])
+    up = glmf.normalize(G[1][:3])
     cam.position[:] = [float(x) for x in eye]
     cam.view[:] = [float(x) for x in view]
     cam.right[:] = [float(x) for x in right]
     cam.up[:] = [float(x) for x in up]
     cam.look_at[:] = [float(x) for x in (eye + view)]
     pi = np.float32(3.1415926535897932384626422832795028841971)
-    yscaled = np.float32(math.tan(np.float32(0.5) * np.float32(fovy) * (pi / np.float32(180))))
+    # float tan / atan of the C math library (the float overloads the loader calls), float
+    # arithmetic around them (scene_load_gltf.cpp:485-491)
+    yscaled = np.float32(_libm().tanf(float(np.float32(0.5) * np.float32(fovy) * (pi / np.float32(180)))))
     xscaled = (yscaled * np.float32(w)) / np.float32(h)
-    cam.fov[:] = [float((np.float32(2) * np.float32(math.atan(xscaled)) * np.float32(180)) / pi), fovy]
+    fovx = (np.float32(2) * np.float32(_libm().atanf(float(xscaled))) * np.float32(180)) / pi
+    cam.fov[:] = [float(fovx), fovy]
     cam.pixel_length[:] = [float(np.float32(2) * xscaled / np.float32(w)), float(np.float32(2) * yscaled / np.float32(h))]
     sb.camera = cam
     return sb

@@ -118,15 +118,18 @@ class SceneBuilder:
         self.textures.append(t)
         return len(self.textures) - 1
 
-    def add_instance(self, mesh: int, material: int, transform=None) -> int:
+    def add_instance(self, mesh: int, material: int, transform=None, inverse=None, inv_transpose=None) -> int:
+        """Place a mesh. Matrices are row-major 4x4; the inverse and inverse transpose are
+        derived in double unless given."""
         M = np.eye(4, dtype=np.float64) if transform is None else np.asarray(transform, np.float64)
-        inv = np.linalg.inv(M)
+        inv = np.linalg.inv(M) if inverse is None else np.asarray(inverse, np.float64)
+        inv_t = inv.T if inv_transpose is None else np.asarray(inv_transpose, np.float64)
         d = InstanceDesc()
         d.mesh, d.material, d.has_inverse = mesh, material, 1
         # column-major (glm) storage
         d.transform[:] = M.T.reshape(-1).astype(np.float32)
         d.inverse[:] = inv.T.reshape(-1).astype(np.float32)
-        d.inv_transpose[:] = inv.reshape(-1).astype(np.float32)
+        d.inv_transpose[:] = inv_t.T.reshape(-1).astype(np.float32)
         self.instances.append(d)
         return len(self.instances) - 1
 

@@ -51,8 +51,9 @@ def compare_descs(a, b):
         ia, ib = a.instances[i], b.instances[i]
         if ia.material != ib.material:
             diffs.append((f"instance {i} material", ia.material, ib.material))
-        if not np.array_equal(np.array(ia.transform), np.array(ib.transform)):
-            diffs.append((f"instance {i} transform", list(ia.transform), list(ib.transform)))
+        for k in ("transform", "inverse", "inv_transpose"):
+            if not np.array_equal(np.array(getattr(ia, k)), np.array(getattr(ib, k))):
+                diffs.append((f"instance {i} {k}", list(getattr(ia, k)), list(getattr(ib, k))))
         ma, mb = mesh_arrays(a, i), mesh_arrays(b, i)
         if set(ma) != set(mb):
             diffs.append((f"instance {i} mesh attributes", sorted(ma), sorted(mb)))
