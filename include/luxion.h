@@ -209,6 +209,24 @@ int lux_scene_free(lux_scene* scene);
 /* Device bytes the scene holds (geometry, BVH, tables, textures). */
 int64_t lux_scene_device_bytes(const lux_scene* scene);
 
+/* Host wall time of the stages of a scene build (no counterpart in the reference). The
+ * geometry (vertex upload, then every BLAS, then instances and TLAS) is built on one thread
+ * while the textures upload on another and the light tables are built on a third. */
+typedef struct lux_scene_stats {
+    double ms_total;          /* the whole build, to the last upload                          */
+    double ms_geometry;       /* upload + BLAS + TLAS                                          */
+    double ms_upload;         /* vertex data to the device                                     */
+    double ms_blas;           /* triangle boxes, every mesh's BVH8, triangle records (device)   */
+    double ms_tlas;           /* instance records, instance boxes, TLAS (device)               */
+    double ms_tables;         /* light CDFs and materials (host)                               */
+    double ms_textures;       /* textures and environment map                                  */
+    int64_t device_bytes;
+    int64_t blas_nodes, tlas_nodes;
+} lux_scene_stats;
+int lux_scene_get_stats(const lux_scene* scene, lux_scene_stats* out);
+/* The same for the scene a context renders (the one lux_init built, or the resident one). */
+int lux_get_scene_stats(lux_ctx* ctx, lux_scene_stats* out);
+
 /* pathtrace: render one sample per pixel. iter is 1-based and seeds the RNG exactly like
  * the reference (include/common.h:38-47). The sample is added to the FP32 accumulation
  * image. If rgba8_dev is not NULL it receives the tonemapped image of the running mean

@@ -38,6 +38,8 @@ SIGNATURES = {
     "lux_init_on_scene": (C.c_int, [_P, C.POINTER(CameraDesc), C.POINTER(Options), C.POINTER(_P)]),
     "lux_scene_free": (C.c_int, [_P]),
     "lux_scene_device_bytes": (C.c_int64, [_P]),
+    "lux_scene_get_stats": (C.c_int, [_P, C.POINTER(_ffi.SceneStats)]),
+    "lux_get_scene_stats": (C.c_int, [_P, C.POINTER(_ffi.SceneStats)]),
     "lux_render_iter": (C.c_int, [_P, C.c_int, _P]),
     "lux_render": (C.c_int, [_P, C.c_int, C.c_int]),
     "lux_copy_image": (C.c_int, [_P, c_float_p]),
@@ -231,6 +233,12 @@ class ResidentScene:
     def device_bytes(self) -> int:
         return int(lib().lux_scene_device_bytes(self._h))
 
+    def build_stats(self) -> dict:
+        """Stage times of the scene build (lux_scene_get_stats)."""
+        st = _ffi.SceneStats()
+        _check(lib().lux_scene_get_stats(self._h, C.byref(st)))
+        return {n: getattr(st, n) for n, _ in _ffi.SceneStats._fields_}
+
     def compatible(self, opt: Options) -> bool:
         """Whether a context with these options can render on this build."""
         return (opt.device, opt.precision, opt.texture_storage) == (
@@ -297,6 +305,12 @@ class Renderer:
         s = Stats()
         _check(lib().lux_get_stats(self._h, C.byref(s)))
         return {n: getattr(s, n) for n, _ in Stats._fields_}
+
+    def scene_stats(self) -> dict:
+        """Stage times of the build of the scene this context renders (lux_get_scene_stats)."""
+        st = _ffi.SceneStats()
+        _check(lib().lux_get_scene_stats(self._h, C.byref(st)))
+        return {n: getattr(st, n) for n, _ in _ffi.SceneStats._fields_}
 
     def copy_image_device(self, dev_ptr: int):
         """Copy the accumulation sum (W*H*3 floats) to device memory at dev_ptr, on the

@@ -100,6 +100,12 @@ class Stats(C.Structure):
         "launches_camera", "launches_accum", "launches_sort", "kernel_launches")]
 
 
+class SceneStats(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("ms_total", "ms_geometry", "ms_upload", "ms_blas", "ms_tlas", "ms_tables",
+                                          "ms_textures")] + \
+        [("device_bytes", C.c_int64), ("blas_nodes", C.c_int64), ("tlas_nodes", C.c_int64)]
+
+
 class RandomSceneParams(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("num_instances", C.c_int32), ("total_tris", C.c_int32),
                 ("min_tris", C.c_int32), ("max_tris", C.c_int32), ("num_emissive", C.c_int32),

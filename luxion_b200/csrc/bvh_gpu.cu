@@ -148,6 +148,7 @@ __global__ void __launch_bounds__(1024) k_chunks(const int* level, int n_level, 
         const int k = (nd.count + kChunk - 1) / kChunk;
         slots[s].chunk0 = c;
         slots[s].nchunk = k;
+        for (int r = 0; r < 12; ++r) slots[s].red[r] = (r < 3 || (r >= 6 && r < 9)) ? 0xffffffffu : 0u;
         for (int j = 0; j < k; ++j) {
             chunk_slot[c + j] = s;
             chunk_start[c + j] = nd.begin + j * kChunk;
@@ -155,19 +156,6 @@ __global__ void __launch_bounds__(1024) k_chunks(const int* level, int n_level, 
         c += k;
     }
     if (threadIdx.x == 1023) *n_chunks = part[1023];
-}
-
-__global__ void k_slot_clear(Slot* slots, int n_level, unsigned* bin_cnt, unsigned* bin_lo, unsigned* bin_hi) {
-    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n_level; s += gridDim.x * blockDim.x) {
-        for (int k = 0; k < 12; ++k) slots[s].red[k] = (k < 3 || (k >= 6 && k < 9)) ? 0xffffffffu : 0u;
-        for (int b = 0; b < 3 * kBins; ++b) {
-            bin_cnt[size_t(s) * 3 * kBins + b] = 0;
-            for (int d = 0; d < 3; ++d) {
-                bin_lo[(size_t(s) * 3 * kBins + b) * 3 + d] = 0xffffffffu;
-                bin_hi[(size_t(s) * 3 * kBins + b) * 3 + d] = 0u;
-            }
-        }
-    }
 }
 
 __device__ __forceinline__ void load_prim(const float* boxes, int p, float* lo, float* hi) {
@@ -294,70 +282,96 @@ __global__ void __launch_bounds__(kBlock) k_bin(const float* boxes, const int* o
 
 // The host builder's sweep over the non-empty bins of each live axis: the first split of
 // lowest cost in (axis, bin) order; no live axis (or a one-sided split) halves the range.
-__global__ void k_split(const int* level, int n_level, const BinNode* bn, Slot* slots, const unsigned* bin_cnt,
-                        const unsigned* bin_lo, const unsigned* bin_hi) {
-    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n_level; s += gridDim.x * blockDim.x) {
+// One warp per node, lane b = bin b: the box and count left of a split after bin b are a
+// prefix union over lanes 0..b, those right of it a suffix union over lanes b+1..31 (empty
+// bins contribute nothing), so every candidate's cost is the host's value exactly.
+constexpr int kSplitWarps = 4;
+__global__ void __launch_bounds__(32 * kSplitWarps) k_split(const int* level, int n_level, const BinNode* bn,
+                                                             Slot* slots, const unsigned* bin_cnt,
+                                                             const unsigned* bin_lo, const unsigned* bin_hi) {
+    const int lane = threadIdx.x & 31;
+    for (int s = blockIdx.x * kSplitWarps + (threadIdx.x >> 5); s < n_level; s += gridDim.x * kSplitWarps) {
         Slot& S = slots[s];
         const BinNode& nd = bn[level[s]];
-        int best_axis = -1, best_split = -1, best_nl = 0;
-        double best_cost = DBL_MAX;
+        double best = DBL_MAX;
+        int bax = 3, bsp = kBins, bnl = 0;
         for (int a = 0; a < 3; ++a) {
             if (!((S.live >> a) & 1)) continue;
-            const size_t g0 = size_t(s) * 3 * kBins + size_t(a) * kBins;
-            // right-side areas and counts after each non-empty bin, accumulated from the top
-            double ra[kBins];
-            int rc[kBins];
-            float acc_lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, acc_hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
-            int cnt = 0;
-            for (int b = kBins - 1; b >= 0; --b) {
-                ra[b] = 0.0;
-                rc[b] = 0;
+            const size_t g = size_t(s) * 3 * kBins + size_t(a) * kBins + lane;
+            const int n = int(bin_cnt[g]);
+            float lo[3], hi[3];
+            for (int d = 0; d < 3; ++d) {
+                lo[d] = n ? fval(bin_lo[g * 3 + d]) : FLT_MAX;
+                hi[d] = n ? fval(bin_hi[g * 3 + d]) : -FLT_MAX;
             }
-            // rights[b]: union of the non-empty bins above b (only read at non-empty b)
-            int last = -1;
-            for (int b = kBins - 1; b >= 0; --b) {
-                const unsigned n = bin_cnt[g0 + b];
-                if (n == 0) continue;
-                if (last >= 0) {
-                    ra[b] = area(acc_lo, acc_hi);
-                    rc[b] = cnt;
-                }
-                for (int d = 0; d < 3; ++d) {
-                    acc_lo[d] = fminf(acc_lo[d], fval(bin_lo[(g0 + b) * 3 + d]));
-                    acc_hi[d] = fmaxf(acc_hi[d], fval(bin_hi[(g0 + b) * 3 + d]));
-                }
-                cnt += int(n);
-                last = b;
+            // inclusive prefix (left side) and inclusive suffix unions over the lanes
+            float pl[3], ph[3], ql[3], qh[3];
+            int pc = n, qc = n;
+            for (int d = 0; d < 3; ++d) {
+                pl[d] = ql[d] = lo[d];
+                ph[d] = qh[d] = hi[d];
             }
-            float l_lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, l_hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
-            int lcnt = 0;
-            int top = -1;  // the last non-empty bin: no split after it
-            for (int b = kBins - 1; b >= 0; --b)
-                if (bin_cnt[g0 + b] != 0) {
-                    top = b;
-                    break;
-                }
-            for (int b = 0; b < top; ++b) {
-                const unsigned n = bin_cnt[g0 + b];
-                if (n == 0) continue;
+            for (int off = 1; off < 32; off <<= 1) {
+                const int uc = __shfl_up_sync(FULL, pc, off), dc = __shfl_down_sync(FULL, qc, off);
+                float ul[3], uh[3], dl[3], dh[3];
                 for (int d = 0; d < 3; ++d) {
-                    l_lo[d] = fminf(l_lo[d], fval(bin_lo[(g0 + b) * 3 + d]));
-                    l_hi[d] = fmaxf(l_hi[d], fval(bin_hi[(g0 + b) * 3 + d]));
+                    ul[d] = __shfl_up_sync(FULL, pl[d], off);
+                    uh[d] = __shfl_up_sync(FULL, ph[d], off);
+                    dl[d] = __shfl_down_sync(FULL, ql[d], off);
+                    dh[d] = __shfl_down_sync(FULL, qh[d], off);
                 }
-                lcnt += int(n);
-                const double c = sah(area(l_lo, l_hi), lcnt, ra[b], rc[b]);
-                if (c < best_cost) {
-                    best_cost = c;
-                    best_axis = a;
-                    best_split = b;
-                    best_nl = lcnt;
+                if (lane >= off) {
+                    pc += uc;
+                    for (int d = 0; d < 3; ++d) {
+                        pl[d] = fminf(pl[d], ul[d]);
+                        ph[d] = fmaxf(ph[d], uh[d]);
+                    }
+                }
+                if (lane + off < 32) {
+                    qc += dc;
+                    for (int d = 0; d < 3; ++d) {
+                        ql[d] = fminf(ql[d], dl[d]);
+                        qh[d] = fmaxf(qh[d], dh[d]);
+                    }
+                }
+            }
+            // right side of a split after bin b: the suffix from b + 1
+            int rc = __shfl_down_sync(FULL, qc, 1);
+            float rl[3], rh[3];
+            for (int d = 0; d < 3; ++d) {
+                rl[d] = __shfl_down_sync(FULL, ql[d], 1);
+                rh[d] = __shfl_down_sync(FULL, qh[d], 1);
+            }
+            if (lane == 31) rc = 0;
+            if (n > 0 && rc > 0) {
+                const double c = sah(area(pl, ph), pc, area(rl, rh), rc);
+                if (c < best) {  // axes ascend, so an earlier axis keeps a tie
+                    best = c;
+                    bax = a;
+                    bsp = lane;
+                    bnl = pc;
                 }
             }
         }
-        if (best_axis >= 0 && (best_nl <= 0 || best_nl >= nd.count)) best_axis = -1;
-        S.axis = best_axis;
-        S.split = best_split;
-        S.nl = best_axis >= 0 ? best_nl : nd.count / 2;
+        for (int off = 16; off > 0; off >>= 1) {
+            const double ob = __shfl_xor_sync(FULL, best, off);
+            const int oa = __shfl_xor_sync(FULL, bax, off);
+            const int os = __shfl_xor_sync(FULL, bsp, off);
+            const int on = __shfl_xor_sync(FULL, bnl, off);
+            if (ob < best || (ob == best && (oa < bax || (oa == bax && os < bsp)))) {
+                best = ob;
+                bax = oa;
+                bsp = os;
+                bnl = on;
+            }
+        }
+        if (lane == 0) {
+            int axis = bax < 3 ? bax : -1;
+            if (axis >= 0 && (bnl <= 0 || bnl >= nd.count)) axis = -1;
+            S.axis = axis;
+            S.split = axis >= 0 ? bsp : -1;
+            S.nl = axis >= 0 ? bnl : nd.count / 2;
+        }
     }
 }
 
@@ -1218,12 +1232,16 @@ int build_bvh8_device(const float* d_boxes, const std::vector<int>& tree_begin, 
         const int grid_s = grid_for(n_level, 128, 4096);
         const int grid_c = std::min(chunk_cap, 148 * 8);
         k_chunks<<<1, 1024, 0, st>>>(large[cur], n_level, bn, slots, chunk_slot, chunk_start, ctr + 4);
-        k_slot_clear<<<grid_s, 128, 0, st>>>(slots, n_level, bin_cnt, bin_lo, bin_hi);
+        // empty bins: count 0, minimum keys all ones, maximum keys zero
+        LUX_CUDA(cudaMemsetAsync(bin_cnt, 0, sizeof(unsigned) * size_t(n_level) * 3 * kBins, st));
+        LUX_CUDA(cudaMemsetAsync(bin_lo, 0xff, sizeof(unsigned) * size_t(n_level) * 3 * kBins * 3, st));
+        LUX_CUDA(cudaMemsetAsync(bin_hi, 0, sizeof(unsigned) * size_t(n_level) * 3 * kBins * 3, st));
         k_reduce<<<grid_c, kBlock, 0, st>>>(d_boxes, ord[cur], large[cur], bn, slots, chunk_slot, chunk_start, ctr + 4);
         k_bin_setup<<<grid_s, 128, 0, st>>>(large[cur], n_level, bn, slots);
         k_bin<<<grid_c, kBlock, 0, st>>>(d_boxes, ord[cur], large[cur], bn, slots, chunk_slot, chunk_start, ctr + 4,
                                           bin_cnt, bin_lo, bin_hi);
-        k_split<<<grid_s, 128, 0, st>>>(large[cur], n_level, bn, slots, bin_cnt, bin_lo, bin_hi);
+        k_split<<<grid_for(n_level, kSplitWarps, 4096), 32 * kSplitWarps, 0, st>>>(large[cur], n_level, bn, slots,
+                                                                                   bin_cnt, bin_lo, bin_hi);
         k_count_left<<<grid_c, kBlock, 0, st>>>(d_boxes, ord[cur], large[cur], bn, slots, chunk_slot, chunk_start,
                                                  ctr + 4, chunk_left);
         k_chunk_base<<<grid_s, 128, 0, st>>>(n_level, slots, chunk_left, chunk_lbase);

@@ -71,6 +71,7 @@ struct lux_scene {
     float h_total_area = 0.0f;
     int64_t instanced_tris = 0;
     size_t scene_bytes = 0;
+    lux_scene_stats stats{};     // stage times of the build
     std::atomic<int> refs{1};
 
     template <class T>
@@ -391,6 +392,7 @@ int lux::build_host_scene(const lux_scene_desc& d, const lux_options& opt, std::
     cudaGetDevice(&dev);
     int tex_rc = LUX_OK;
     std::string tex_err;
+    const auto t0 = std::chrono::steady_clock::now();
     std::thread texer([&]() {
         if (cudaSetDevice(dev) != cudaSuccess) {
             tex_rc = fail(LUX_ERR_CUDA, "cudaSetDevice failed on the texture thread");
@@ -407,6 +409,7 @@ int lux::build_host_scene(const lux_scene_desc& d, const lux_options& opt, std::
                                       stage);
             }
         }
+        H.ms_textures = ms_since(t0);
         if (tex_rc == LUX_OK && device_work) tex_rc = device_work();
         if (tex_rc) tex_err = g_err;
     });
@@ -453,6 +456,7 @@ int lux::build_host_scene(const lux_scene_desc& d, const lux_options& opt, std::
         return fail(LUX_ERR_INVALID, "-dmis requires the scene to contain emissive geometry");
     if (opt.env_importance_sampling && !d.env_data)
         return fail(LUX_ERR_INVALID, "-emis requires an environment map");
+    H.ms_tables = ms_since(t0);
     // ---- materials + textures ----
     texer.join();
     if (tex_rc) return fail(tex_rc, tex_err);
@@ -525,6 +529,7 @@ namespace {
 
 // Host build and upload of the scene; device_work runs on the build's device thread.
 int build_scene(lux_scene* R, const lux_scene_desc& d, const lux_options& opt, const std::function<int()>& device_work) {
+    const auto t_start = std::chrono::steady_clock::now();
     // The device geometry (vertex uploads, every BVH) is built on its own thread and stream,
     // while this thread builds the light tables and the texture thread uploads the textures.
     const int dev = R->device;
@@ -552,6 +557,15 @@ int build_scene(lux_scene* R, const lux_scene_desc& d, const lux_options& opt, c
     if (rc) return rc;
     if (geo_rc) return fail(geo_rc, geo_err);
     R->instanced_tris = G.instanced_tris[0];
+    lux_scene_stats& st = R->stats;
+    st.ms_geometry = G.ms_total;
+    st.ms_upload = G.ms_upload;
+    st.ms_blas = G.ms_blas;
+    st.ms_tlas = G.ms_tlas;
+    st.ms_tables = H.ms_tables;
+    st.ms_textures = H.ms_textures;
+    st.blas_nodes = int64_t(G.blas_nodes);
+    st.tlas_nodes = int64_t(G.tlas_nodes);
     R->h_emissive_prefix = H.emissive_prefix;
     R->h_tri_prefix = H.tri_prefix;
     R->h_marginal = H.marginal;
@@ -562,7 +576,10 @@ int build_scene(lux_scene* R, const lux_scene_desc& d, const lux_options& opt, c
     R->scene_bytes += R->env.bytes;
     R->S = geo;
     if ((rc = upload_scene_materials(R, H, R->S))) return rc;
-    return upload_scene_lights(R, H, R->S);
+    if ((rc = upload_scene_lights(R, H, R->S))) return rc;
+    st.ms_total = ms_since(t_start);
+    st.device_bytes = int64_t(R->scene_bytes);
+    return LUX_OK;
 }
 
 void scene_release(lux_scene* R) {
@@ -987,6 +1004,18 @@ int lux_scene_free(lux_scene* scene) {
 }
 
 int64_t lux_scene_device_bytes(const lux_scene* scene) { return scene ? int64_t(scene->scene_bytes) : 0; }
+
+int lux_scene_get_stats(const lux_scene* scene, lux_scene_stats* out) {
+    if (!scene || !out) return fail(LUX_ERR_INVALID, "NULL argument");
+    *out = scene->stats;
+    return LUX_OK;
+}
+
+int lux_get_scene_stats(lux_ctx* C, lux_scene_stats* out) {
+    if (!C || !out) return fail(LUX_ERR_INVALID, "NULL argument");
+    *out = C->scene->stats;
+    return LUX_OK;
+}
 
 int lux_init_on_scene(lux_scene* R, const lux_camera_desc* camera, const lux_options* opt, lux_ctx** out) {
     if (!out) return fail(LUX_ERR_INVALID, "out is NULL");

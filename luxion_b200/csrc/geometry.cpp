@@ -68,6 +68,7 @@ struct Scratch {
 
 int build_geometry(const lux_scene_desc* const* scenes, int ns, const std::vector<int>& material_base,
                    const DevAlloc& alloc, cudaStream_t st, DevScene& S, GeometryBuild& G) {
+    const auto t0 = std::chrono::steady_clock::now();
     // ---- offsets of the concatenation ----
     std::vector<int> mesh_base(size_t(ns) + 1, 0);
     G.inst_base.assign(size_t(ns) + 1, 0);
@@ -120,6 +121,8 @@ int build_geometry(const lux_scene_desc* const* scenes, int ns, const std::vecto
         }
     }
 
+    LUX_CUDA(cudaStreamSynchronize(st));
+    G.ms_upload = ms_since(t0);
     // ---- BLAS of every mesh ----
     Scratch X;
     uint32_t *d_tri_off = nullptr, *d_vert_off = nullptr;
@@ -143,6 +146,8 @@ int build_geometry(const lux_scene_desc* const* scenes, int ns, const std::vecto
     if (int rc = own(&prims, T * 3, sizeof(float4))) return rc;
     LUX_CUDA(launch_tri_records(blas.leaf_prim, int(T), prim_mesh, d_tri_off, d_vert_off, pos, idx, prims, st));
 
+    LUX_CUDA(cudaStreamSynchronize(st));
+    G.ms_blas = ms_since(t0) - G.ms_upload;
     // ---- instances ----
     std::vector<DevInstance> insts(NI);
     std::vector<float> M12(size_t(NI) * 12);
@@ -256,6 +261,8 @@ int build_geometry(const lux_scene_desc* const* scenes, int ns, const std::vecto
     LUX_CUDA(cudaMemcpyAsync(tlas_leaf, leaf.data(), sizeof(float4) * leaf.size(), cudaMemcpyHostToDevice, st));
     LUX_CUDA(cudaStreamSynchronize(st));
 
+    G.ms_total = ms_since(t0);
+    G.ms_tlas = G.ms_total - G.ms_upload - G.ms_blas;
     S.nodes = reinterpret_cast<const uint4*>(nodes);
     S.prims = prims;
     S.insts = d_insts;

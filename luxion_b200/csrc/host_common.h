@@ -12,6 +12,7 @@
 #include <cstdint>
 #include <cstring>
 #include <algorithm>
+#include <chrono>
 #include <functional>
 #include <string>
 #include <vector>
@@ -21,6 +22,10 @@ namespace lux {
 extern thread_local std::string g_err;
 // record msg for lux_last_error() and return code
 int fail(int code, const std::string& msg);
+
+inline double ms_since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
 
 #define LUX_CUDA(call)                                                                      \
     do {                                                                                    \
@@ -97,6 +102,7 @@ struct HostScene {
     unsigned long long env_tex = 0;
     bool has_env = false;
     float morton_bmin[3] = {0, 0, 0}, morton_bmax[3] = {0, 0, 0};
+    double ms_tables = 0, ms_textures = 0;  // light tables + materials; texture thread
 };
 
 // Device allocation that the owner records (and frees with everything else it owns).
@@ -109,6 +115,7 @@ struct GeometryBuild {
     std::vector<int> inst_base;           // per scene (+ total): first instance in the concatenation
     std::vector<int> max_blas_depth;      // per scene
     uint32_t blas_nodes = 0, tlas_nodes = 0;
+    double ms_upload = 0, ms_blas = 0, ms_tlas = 0, ms_total = 0;  // host wall time per stage
     size_t bytes = 0;                     // device bytes allocated through alloc
 };
 

@@ -42,7 +42,7 @@ STRUCTS = {
     "lux_scene_desc": _ffi.SceneDesc, "lux_options": _ffi.Options, "lux_stats": _ffi.Stats,
     "lux_random_scene_params": _ffi.RandomSceneParams, "lux_job_desc": _ffi.JobDesc,
     "lux_engine_config": _ffi.EngineConfig, "lux_job_status": _ffi.JobStatus,
-    "lux_engine_stats": _ffi.EngineStats,
+    "lux_engine_stats": _ffi.EngineStats, "lux_scene_stats": _ffi.SceneStats,
 }
 
 

@@ -50,7 +50,11 @@ def loaded():
 
 
 def quat(x, y, z, w):
-    return gltf._quat_mat(x, y, z, w)
+    """Rotation matrix of the unit quaternion (x, y, z, w), in double (row-major)."""
+    return np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y), 0],
+                     [2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x), 0],
+                     [2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y), 0],
+                     [0, 0, 0, 1]], np.float64)
 
 
 def test_materials(loaded):
