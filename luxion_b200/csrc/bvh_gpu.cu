@@ -22,8 +22,48 @@
 
 #include <cfloat>
 #include <cmath>
+#include <map>
+#include <mutex>
 
 namespace lux {
+
+// Scratch of the device builds comes from one memory pool per device, owned by the library:
+// allocations and frees are stream-ordered (no device-wide synchronisation, as cudaFree has),
+// and up to kPoolKeep bytes of freed scratch stay reserved for the next build.
+namespace {
+constexpr uint64_t kPoolKeep = uint64_t(4) << 30;
+std::mutex g_pool_mu;
+std::map<int, cudaMemPool_t> g_pools;
+}  // namespace
+
+cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t st) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    cudaMemPool_t pool;
+    {
+        std::lock_guard<std::mutex> lock(g_pool_mu);
+        auto it = g_pools.find(dev);
+        if (it == g_pools.end()) {
+            cudaMemPoolProps props{};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            if ((e = cudaMemPoolCreate(&pool, &props)) != cudaSuccess) return e;
+            uint64_t keep = kPoolKeep;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+            g_pools[dev] = pool;
+        } else {
+            pool = it->second;
+        }
+    }
+    return cudaMallocFromPoolAsync(p, bytes, pool, st);
+}
+
+void scratch_free(void* p, cudaStream_t st) {
+    if (p) cudaFreeAsync(p, st);
+}
+
 namespace {
 
 constexpr int kBins = 32;
@@ -1135,14 +1175,16 @@ __global__ void k_inst_boxes(const float* M, const int* inst_mesh, int num_insts
 
 // device buffers of one build, freed together
 struct Bufs {
+    cudaStream_t st;
     std::vector<void*> p;
+    explicit Bufs(cudaStream_t s) : st(s) {}
     ~Bufs() {
-        for (void* q : p) cudaFree(q);
+        for (void* q : p) scratch_free(q, st);
     }
     template <class T>
     T* get(size_t n) {
         void* q = nullptr;
-        if (cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) return nullptr;
+        if (scratch_alloc(&q, std::max<size_t>(n, 1) * sizeof(T), st) != cudaSuccess) return nullptr;
         p.push_back(q);
         return static_cast<T*>(q);
     }
@@ -1163,8 +1205,8 @@ int device_scan(const int* in, int n, int* out, int* total, int* block_sums, cud
 }  // namespace
 
 void DeviceBvh8::release() {
-    if (nodes) cudaFree(nodes);
-    if (leaf_prim) cudaFree(leaf_prim);
+    scratch_free(nodes, stream);
+    scratch_free(leaf_prim, stream);
     nodes = nullptr;
     leaf_prim = nullptr;
     num_nodes = 0;
@@ -1178,7 +1220,7 @@ int build_bvh8_device(const float* d_boxes, const std::vector<int>& tree_begin, 
     for (int t = 0; t < G; ++t)
         if (tree_begin[t + 1] <= tree_begin[t]) return fail(LUX_ERR_INVALID, "BVH build: a tree without primitives");
     const int N = tree_begin[G];
-    Bufs B;
+    Bufs B(st);
     int* d_tb = B.get<int>(G + 1);
     int* ord[2] = {B.get<int>(N), B.get<int>(N)};
     int* ord_fin = B.get<int>(N);
@@ -1334,8 +1376,10 @@ int build_bvh8_device(const float* d_boxes, const std::vector<int>& tree_begin, 
     k_tree_offsets<<<1, 1024, 0, st>>>(G, L, first, last, lsp, nlp, node_base, node_off, leaf_off, tree_nodes,
                                        tree_depth, tree_root);
     LUX_CUDA(cudaGetLastError());
-    if (cudaMalloc(&out.nodes, sizeof(BVH8Node) * std::max<size_t>(total_items, 1)) != cudaSuccess ||
-        cudaMalloc(&out.leaf_prim, sizeof(uint32_t) * size_t(N)) != cudaSuccess) {
+    out.stream = st;
+    if (scratch_alloc(reinterpret_cast<void**>(&out.nodes), sizeof(BVH8Node) * std::max<size_t>(total_items, 1), st) !=
+            cudaSuccess ||
+        scratch_alloc(reinterpret_cast<void**>(&out.leaf_prim), sizeof(uint32_t) * size_t(N), st) != cudaSuccess) {
         out.release();
         return fail(LUX_ERR_OOM, "BVH build: node allocation failed");
     }

@@ -26,12 +26,18 @@ struct DeviceBvh8 {
     std::vector<uint32_t> root;     // per tree: node index of its root (node_base added)
     std::vector<uint32_t> count;    // per tree: nodes
     std::vector<int> depth;         // per tree: 8-wide levels (root = 1)
+    cudaStream_t stream = nullptr;  // the build's stream: the arrays are freed on it
     DeviceBvh8() = default;
     DeviceBvh8(const DeviceBvh8&) = delete;
     DeviceBvh8& operator=(const DeviceBvh8&) = delete;
     ~DeviceBvh8() { release(); }
     void release();
 };
+
+// Stream-ordered scratch from the library's per-device memory pool (freed scratch stays
+// reserved for the next build, up to a few GB).
+cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t st);
+void scratch_free(void* p, cudaStream_t st);
 
 // Build over n = tree_begin.back() primitive boxes (d_boxes: device, n * 6 floats, min xyz then
 // max xyz, padded by the caller). Tree t owns primitives [tree_begin[t], tree_begin[t+1]); it

@@ -47,17 +47,19 @@ bool invert4(const float* m, double* out) {
     return true;
 }
 
-// Scratch device memory of one geometry build.
+// Scratch device memory of one geometry build (stream-ordered, from the build pool).
 struct Scratch {
+    cudaStream_t st;
     std::vector<void*> p;
+    explicit Scratch(cudaStream_t s) : st(s) {}
     ~Scratch() {
-        for (void* q : p) cudaFree(q);
+        for (void* q : p) scratch_free(q, st);
     }
     template <class T>
     int get(T** out, size_t n) {
         void* q = nullptr;
-        cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T));
-        if (e != cudaSuccess) return fail(LUX_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        cudaError_t e = scratch_alloc(&q, std::max<size_t>(n, 1) * sizeof(T), st);
+        if (e != cudaSuccess) return fail(LUX_ERR_OOM, std::string("scratch allocation: ") + cudaGetErrorString(e));
         p.push_back(q);
         *out = static_cast<T*>(q);
         return LUX_OK;
@@ -124,7 +126,7 @@ int build_geometry(const lux_scene_desc* const* scenes, int ns, const std::vecto
     LUX_CUDA(cudaStreamSynchronize(st));
     G.ms_upload = ms_since(t0);
     // ---- BLAS of every mesh ----
-    Scratch X;
+    Scratch X(st);
     uint32_t *d_tri_off = nullptr, *d_vert_off = nullptr;
     int* prim_mesh = nullptr;
     float *boxes = nullptr, *mesh_box = nullptr;
@@ -318,7 +320,7 @@ extern "C" int lux_bvh8_build(const float* boxes, const int* tree_begin, int num
         cudaStream_t s;
         ~StreamFree() { cudaStreamDestroy(s); }
     } sf{st};
-    Scratch X;
+    Scratch X(st);
     float* d_boxes = nullptr;
     if (int rc = X.get(&d_boxes, size_t(n) * 6)) return rc;
     LUX_CUDA(cudaMemcpyAsync(d_boxes, boxes, sizeof(float) * 6 * size_t(n), cudaMemcpyHostToDevice, st));
