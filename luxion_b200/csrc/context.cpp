@@ -16,6 +16,7 @@
 
 #include "../../include/luxion.h"
 #include "bvh8.h"
+#include "bvh_gpu.h"
 #include "device_scene.h"
 #include "launch.h"
 #include "host_common.h"
@@ -121,11 +122,17 @@ struct lux_ctx {
     cudaEvent_t ev[2] = {nullptr, nullptr};
     std::vector<cudaEvent_t> kev;
 
+    // per-pixel and per-path state: stream-ordered from the library's device memory pool, so
+    // a context is made and freed without device-wide synchronisation, and the next context
+    // reuses the memory (the reference's pathtraceFree / pathtraceInit on every reset)
     template <class T>
     int alloc(T** p, size_t n) {
-        int rc = dalloc(p, n);
-        if (rc == LUX_OK && *p) allocs.push_back(*p);
-        return rc;
+        *p = nullptr;
+        if (n == 0) return LUX_OK;
+        cudaError_t e = scratch_alloc(reinterpret_cast<void**>(p), n * sizeof(T), stream);
+        if (e != cudaSuccess) return fail(LUX_ERR_OOM, std::string("device allocation: ") + cudaGetErrorString(e));
+        allocs.push_back(*p);
+        return LUX_OK;
     }
 };
 
@@ -1157,7 +1164,7 @@ int lux_free(lux_ctx* C) {
     cudaSetDevice(C->device);
     if (C->stream) cudaStreamSynchronize(C->stream);
     for (auto& g : C->graphs) cudaGraphExecDestroy(g.second);
-    for (void* p : C->allocs) cudaFree(p);
+    for (void* p : C->allocs) scratch_free(p, C->stream);
     if (C->h_wave_iter) cudaFreeHost(C->h_wave_iter);
     if (C->h_ctr) cudaFreeHost(C->h_ctr);
     for (auto e : C->kev) cudaEventDestroy(e);
