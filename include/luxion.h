@@ -179,7 +179,17 @@ typedef struct lux_options {
                                           * debug_bvh, src/kernels/draw_bvh.cu:6-35): each
                                           * sample adds (BVH8 node visits + triangle tests)
                                           * * 0.001 to every channel of its pixel             */
+    int32_t bvh_layout;                  /* LUX_BVH_*: how a scene build lays out its BVH     */
 } lux_options;
+
+/* BVH layout of a scene build. Both give the same hits bit for bit (every triangle is tested
+ * in its instance's object space, as the reference does, src/intersections/mesh_isect.cu:15-16):
+ * SINGLE_LEVEL builds one world-space BVH per scene over all instanced triangles, so traversal
+ * never switches instances; TWO_LEVEL builds one BLAS per mesh and a TLAS over the instances
+ * (the reference's GAS/IAS structure), which keeps one copy of a mesh that many instances
+ * share. AUTO takes SINGLE_LEVEL unless the instanced triangles are both more than twice the
+ * meshes' and more than 16M. */
+enum { LUX_BVH_AUTO = 0, LUX_BVH_TWO_LEVEL = 1, LUX_BVH_SINGLE_LEVEL = 2 };
 
 typedef struct lux_ctx lux_ctx;
 typedef struct lux_scene lux_scene;
@@ -194,8 +204,9 @@ int lux_init(const lux_scene_desc* scene, const lux_options* opt, lux_ctx** out)
 /* A resident scene: geometry, BVH, materials, textures and light CDFs on one device, built
  * once. The reference does this work at load, before the first pathtraceInit: mesh uploads and
  * acceleration builds in main() (src/main.cpp:199-274) and the light precompute
- * (src/scene/scene_precompute.cpp:22-124). Of the options only device, texture_storage and
- * precision shape the build; every context made on the scene must use the same three. */
+ * (src/scene/scene_precompute.cpp:22-124). Of the options only device, texture_storage,
+ * precision and bvh_layout shape the build; every context made on the scene must use the same
+ * device, texture_storage and precision. */
 int lux_scene_create(const lux_scene_desc* scene, const lux_options* opt, lux_scene** out);
 /* pathtraceInit on a resident scene (src/pathtrace/pathtrace_buffers.cu:21-140): allocate only
  * the per-pixel and per-path state for `camera` (any resolution; NULL = the description's

@@ -84,13 +84,17 @@ class SceneDesc(C.Structure):
                 ("env_data", C.c_void_p)]
 
 
+BVH_AUTO, BVH_TWO_LEVEL, BVH_SINGLE_LEVEL = 0, 1, 2
+
+
 class Options(C.Structure):
     _fields_ = [("direct_light_sampling", C.c_int32), ("env_importance_sampling", C.c_int32),
                 ("color_mode", C.c_int32), ("envmap_intensity", C.c_float),
                 ("trace_depth", C.c_int32), ("ray_sorting", C.c_int32),
                 ("precision", C.c_int32), ("spp_per_wave", C.c_int32),
                 ("use_graph", C.c_int32), ("texture_storage", C.c_int32), ("device", C.c_int32),
-                ("stream", C.c_void_p), ("material_debug_mode", C.c_int32), ("debug_bvh", C.c_int32)]
+                ("stream", C.c_void_p), ("material_debug_mode", C.c_int32), ("debug_bvh", C.c_int32),
+                ("bvh_layout", C.c_int32)]
 
 
 class Stats(C.Structure):
@@ -154,6 +158,7 @@ def default_options(**kw) -> Options:
     o.spp_per_wave = 0
     o.use_graph = 1
     o.texture_storage = TEXSTORE_FLOAT
+    o.bvh_layout = BVH_AUTO
     o.device = 0
     o.stream = None
     o.material_debug_mode = MATDEBUG_OFF

@@ -1173,6 +1173,69 @@ __global__ void k_inst_boxes(const float* M, const int* inst_mesh, int num_insts
     }
 }
 
+// World boxes of instanced triangles for the single-level layout: flat primitive f is
+// triangle k = f - inst_tri_off[i] of instance i = flat_inst[f]. The box of the triangle's
+// vertices transformed in double is padded by 1e-5 of the instance's world extent plus 1e-5 of
+// its largest coordinate (ibox: the instance's padded world box): the object-space triangle
+// test sees the ray through the instance's float inverse, whose point error grows with the
+// coordinates' magnitude, and the pad covers it for condition numbers up to about 20.
+__global__ void k_flat_boxes(const float* M, const int* inst_mesh, const uint32_t* inst_tri_off, const int* flat_inst,
+                             int n, const float* ibox, const float* pos, const uint32_t* idx, const uint32_t* tri_off,
+                             const uint32_t* vert_off, float* boxes) {
+    for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < n; f += gridDim.x * blockDim.x) {
+        const int i = flat_inst[f];
+        const int m = inst_mesh[i];
+        const uint32_t p = tri_off[m] + (uint32_t(f) - inst_tri_off[i]);
+        const float* T = M + size_t(i) * 12;
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+        for (int c = 0; c < 3; ++c) {
+            const float* v = pos + size_t(vert_off[m] + idx[size_t(p) * 3 + c]) * 3;
+            for (int a = 0; a < 3; ++a) {
+                const double w = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(double(T[0 * 3 + a]), double(v[0])),
+                                                               __dmul_rn(double(T[1 * 3 + a]), double(v[1]))),
+                                                     __dmul_rn(double(T[2 * 3 + a]), double(v[2]))),
+                                           double(T[3 * 3 + a]));
+                lo[a] = fmin(lo[a], w);
+                hi[a] = fmax(hi[a], w);
+            }
+        }
+        const float* ib = ibox + size_t(i) * 6;
+        double mext = 0.0, mabs = 0.0;
+        for (int a = 0; a < 3; ++a) {
+            mext = fmax(mext, __dsub_rn(double(ib[3 + a]), double(ib[a])));
+            mabs = fmax(mabs, fmax(fabs(double(ib[a])), fabs(double(ib[3 + a]))));
+        }
+        const double pad = __dadd_rn(__dmul_rn(1e-5, __dadd_rn(mext, mabs)), 1e-12);
+        for (int a = 0; a < 3; ++a) {
+            boxes[size_t(f) * 6 + a] = __double2float_rd(__dsub_rn(lo[a], pad));
+            boxes[size_t(f) * 6 + 3 + a] = __double2float_ru(__dadd_rn(hi[a], pad));
+        }
+    }
+}
+
+// Single-level triangle records in leaf order: v0 with the mesh-local triangle index in w,
+// e1 with the instance index in w, e2 -- object-space values, exactly those of the two-level
+// records, so the triangle test is the same.
+__global__ void k_flat_records(const uint32_t* leaf_prim, int n, const int* flat_inst, const uint32_t* inst_tri_off,
+                               const int* inst_mesh, const uint32_t* tri_off, const uint32_t* vert_off, const float* pos,
+                               const uint32_t* idx, float4* out) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        const uint32_t f = min(leaf_prim[r], uint32_t(n - 1));
+        const int i = flat_inst[f];
+        const int m = inst_mesh[i];
+        const uint32_t k = f - inst_tri_off[i];
+        const uint32_t p = tri_off[m] + k;
+        const uint32_t vb = vert_off[m];
+        const float* v0 = pos + size_t(vb + idx[size_t(p) * 3 + 0]) * 3;
+        const float* v1 = pos + size_t(vb + idx[size_t(p) * 3 + 1]) * 3;
+        const float* v2 = pos + size_t(vb + idx[size_t(p) * 3 + 2]) * 3;
+        out[size_t(r) * 3 + 0] = make_float4(v0[0], v0[1], v0[2], __int_as_float(int(k)));
+        out[size_t(r) * 3 + 1] = make_float4(__fsub_rn(v1[0], v0[0]), __fsub_rn(v1[1], v0[1]), __fsub_rn(v1[2], v0[2]),
+                                             __int_as_float(i));
+        out[size_t(r) * 3 + 2] = make_float4(__fsub_rn(v2[0], v0[0]), __fsub_rn(v2[1], v0[1]), __fsub_rn(v2[2], v0[2]), 0.0f);
+    }
+}
+
 // device buffers of one build, freed together
 struct Bufs {
     cudaStream_t st;
@@ -1420,6 +1483,24 @@ cudaError_t launch_tri_records(const uint32_t* leaf_prim, int n, const int* prim
                                cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
     k_tri_records<<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(leaf_prim, n, prim_mesh, tri_off, vert_off, pos, idx, prims);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_flat_boxes(const float* M, const int* inst_mesh, const uint32_t* inst_tri_off, const int* flat_inst,
+                              int n, const float* ibox, const float* pos, const uint32_t* idx, const uint32_t* tri_off,
+                              const uint32_t* vert_off, float* boxes, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    k_flat_boxes<<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(M, inst_mesh, inst_tri_off, flat_inst, n, ibox, pos, idx,
+                                                             tri_off, vert_off, boxes);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_flat_records(const uint32_t* leaf_prim, int n, const int* flat_inst, const uint32_t* inst_tri_off,
+                                const int* inst_mesh, const uint32_t* tri_off, const uint32_t* vert_off, const float* pos,
+                                const uint32_t* idx, float4* prims, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    k_flat_records<<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(leaf_prim, n, flat_inst, inst_tri_off, inst_mesh, tri_off,
+                                                               vert_off, pos, idx, prims);
     return cudaGetLastError();
 }
 

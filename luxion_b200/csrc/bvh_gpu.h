@@ -66,6 +66,16 @@ cudaError_t launch_tri_records(const uint32_t* leaf_prim, int n, const int* prim
 cudaError_t launch_inst_boxes(const float* M, const int* inst_mesh, int num_insts, const float* pos,
                               const uint32_t* vert_off, const float* mesh_box, int exact, float* boxes,
                               cudaStream_t st);
+// Single-level layout: padded world boxes of instanced triangles (flat primitive f is triangle
+// f - inst_tri_off[i] of instance i = flat_inst[f]; ibox: the instances' padded world boxes),
+// and the triangle records in leaf order (object-space v0 / e1 / e2 of the triangle, its
+// mesh-local index in v0.w, its instance in e1.w).
+cudaError_t launch_flat_boxes(const float* M, const int* inst_mesh, const uint32_t* inst_tri_off, const int* flat_inst,
+                              int n, const float* ibox, const float* pos, const uint32_t* idx, const uint32_t* tri_off,
+                              const uint32_t* vert_off, float* boxes, cudaStream_t st);
+cudaError_t launch_flat_records(const uint32_t* leaf_prim, int n, const int* flat_inst, const uint32_t* inst_tri_off,
+                                const int* inst_mesh, const uint32_t* tri_off, const uint32_t* vert_off, const float* pos,
+                                const uint32_t* idx, float4* prims, cudaStream_t st);
 // Float box of each mesh's vertices (6 floats per mesh).
 cudaError_t launch_mesh_boxes(const float* pos, const uint32_t* vert_off, int num_meshes, float* boxes,
                               cudaStream_t st);

@@ -552,7 +552,7 @@ int build_scene(lux_scene* R, const lux_scene_desc& d, const lux_options& opt, c
             return;
         }
         const lux_scene_desc* one = &d;
-        geo_rc = build_geometry(&one, 1, std::vector<int>{0},
+        geo_rc = build_geometry(&one, 1, std::vector<int>{0}, opt.bvh_layout,
                                 [&](void** p, size_t bytes) { return R->alloc(reinterpret_cast<char**>(p), bytes); },
                                 st, geo, G);
         if (geo_rc) geo_err = g_err;
@@ -604,6 +604,8 @@ int check_options_and_device(const lux_options& o) {
         return fail(LUX_ERR_INVALID, "unknown texture storage");
     if (o.precision != LUX_PRECISION_PLAIN && o.precision != LUX_PRECISION_COMPENSATED)
         return fail(LUX_ERR_INVALID, "unknown precision");
+    if (o.bvh_layout < LUX_BVH_AUTO || o.bvh_layout > LUX_BVH_SINGLE_LEVEL)
+        return fail(LUX_ERR_INVALID, "unknown BVH layout");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(LUX_ERR_NO_DEVICE, "no CUDA device");
     if (o.device < 0 || o.device >= ndev) return fail(LUX_ERR_INVALID, "device ordinal out of range");
@@ -972,7 +974,7 @@ int ctx_finish(lux_ctx* C) {
     if (cudaEventCreate(&C->ev[0]) != cudaSuccess || cudaEventCreate(&C->ev[1]) != cudaSuccess)
         return fail(LUX_ERR_CUDA, "cudaEventCreate failed");
     // occupancy queries happen here, never inside a stream capture
-    for (int m = 0; m < 4; ++m) trace_grid_blocks(m);
+    for (int m = 0; m < 4; ++m) trace_grid_blocks(m, C->S.single_level != 0);
     shade_grid_blocks();
     if (cudaStreamSynchronize(C->stream) != cudaSuccess) return fail(LUX_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
     if (cudaGetLastError() != cudaSuccess) return fail(LUX_ERR_CUDA, "context set-up failed");

@@ -73,6 +73,10 @@ struct DevScene {
     const float4* tlas_leaf;
     uint32_t tlas_root;
     int num_insts;
+    // 1: nodes under tlas_root are one world-space BVH over instanced triangles; its leaf
+    // records carry their instance in e1.w and are tested in that instance's object space.
+    // 0: two levels, a TLAS over instances (tlas_leaf records) above per-mesh BLASes.
+    int single_level;
     const float* pos;
     const float* nrm;
     const float* uv;

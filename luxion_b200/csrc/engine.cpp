@@ -244,6 +244,8 @@ int lux_engine_create(const lux_scene_desc* const* scenes, int num_scenes, const
     else lux_default_options(&o);
     if (o.texture_storage < LUX_TEXSTORE_FLOAT || o.texture_storage > LUX_TEXSTORE_HALF)
         return fail(LUX_ERR_INVALID, "unknown texture storage");
+    if (o.bvh_layout < LUX_BVH_AUTO || o.bvh_layout > LUX_BVH_SINGLE_LEVEL)
+        return fail(LUX_ERR_INVALID, "unknown BVH layout");
     if (o.material_debug_mode || o.debug_bvh)
         return fail(LUX_ERR_UNSUPPORTED, "debug views are rendered by lux_init contexts, not by the engine");
     lux_engine_config c{};
@@ -286,7 +288,7 @@ int lux_engine_create(const lux_scene_desc* const* scenes, int num_scenes, const
     std::vector<int> mat_base(num_scenes, 0);
     for (int i = 1; i < num_scenes; ++i) mat_base[i] = mat_base[i - 1] + scenes[i - 1]->num_materials;
     GeometryBuild G;
-    if (int rc = build_geometry(scenes, num_scenes, mat_base,
+    if (int rc = build_geometry(scenes, num_scenes, mat_base, o.bvh_layout,
                                 [&](void** p, size_t bytes) { return E->up_alloc(reinterpret_cast<char**>(p), bytes); },
                                 E->stream, E->S, G))
         return bail(rc);
@@ -344,9 +346,9 @@ int lux_engine_create(const lux_scene_desc* const* scenes, int num_scenes, const
     cudaEventCreate(&E->ev[0]);
     cudaEventCreate(&E->ev[1]);
     // occupancy queries happen here, never inside a stream capture
-    for (int m = 0; m < 3; ++m) trace_grid_blocks(m);
+    for (int m = 0; m < 3; ++m) trace_grid_blocks(m, E->S.single_level != 0);
     shade_grid_blocks();
-    const int full = trace_grid_blocks(0);
+    const int full = trace_grid_blocks(0, E->S.single_level != 0);
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, E->device);
     if (c.max_paths > 0 || c.trace_blocks > 0) {

@@ -68,7 +68,7 @@ struct Scratch {
 
 }  // namespace
 
-int build_geometry(const lux_scene_desc* const* scenes, int ns, const std::vector<int>& material_base,
+int build_geometry(const lux_scene_desc* const* scenes, int ns, const std::vector<int>& material_base, int layout,
                    const DevAlloc& alloc, cudaStream_t st, DevScene& S, GeometryBuild& G) {
     const auto t0 = std::chrono::steady_clock::now();
     // ---- offsets of the concatenation ----
@@ -93,6 +93,16 @@ int build_geometry(const lux_scene_desc* const* scenes, int ns, const std::vecto
         any_uv |= mesh[m]->uvs != nullptr;
     }
     const size_t T = tri_off[NM], V = vert_off[NM];
+    // Layout: the single-level world BVH (no instance transitions during traversal) unless
+    // instancing makes its per-instance triangle records large: more than 2x the meshes'
+    // triangles and more than 16M of them.
+    size_t instanced = 0;
+    for (int s = 0; s < ns; ++s)
+        for (int i = 0; i < scenes[s]->num_instances; ++i)
+            instanced += size_t(mesh[mesh_base[s] + scenes[s]->instances[i].mesh]->num_tris);
+    if (instanced >= (size_t(1) << 31)) return fail(LUX_ERR_UNSUPPORTED, "more than 2^31 instanced triangles");
+    const bool flat = layout == LUX_BVH_SINGLE_LEVEL ||
+                      (layout == LUX_BVH_AUTO && (instanced <= 2 * T || instanced <= (size_t(16) << 20)));
     G.bytes = 0;
     auto own = [&](auto** p, size_t n, size_t elem) -> int {
         G.bytes += n * elem;
@@ -125,29 +135,29 @@ int build_geometry(const lux_scene_desc* const* scenes, int ns, const std::vecto
 
     LUX_CUDA(cudaStreamSynchronize(st));
     G.ms_upload = ms_since(t0);
-    // ---- BLAS of every mesh ----
+    // ---- BLAS of every mesh (two-level layout) ----
     Scratch X(st);
     uint32_t *d_tri_off = nullptr, *d_vert_off = nullptr;
-    int* prim_mesh = nullptr;
-    float *boxes = nullptr, *mesh_box = nullptr;
+    float* mesh_box = nullptr;
     if (int rc = X.get(&d_tri_off, size_t(NM) + 1)) return rc;
     if (int rc = X.get(&d_vert_off, size_t(NM) + 1)) return rc;
-    if (int rc = X.get(&prim_mesh, T)) return rc;
-    if (int rc = X.get(&boxes, T * 6)) return rc;
     if (int rc = X.get(&mesh_box, size_t(NM) * 6)) return rc;
     LUX_CUDA(cudaMemcpyAsync(d_tri_off, tri_off.data(), sizeof(uint32_t) * (NM + 1), cudaMemcpyHostToDevice, st));
     LUX_CUDA(cudaMemcpyAsync(d_vert_off, vert_off.data(), sizeof(uint32_t) * (NM + 1), cudaMemcpyHostToDevice, st));
-    LUX_CUDA(launch_fill_mesh_ids(d_tri_off, NM, prim_mesh, st));
-    LUX_CUDA(launch_tri_boxes(pos, idx, prim_mesh, d_vert_off, int(T), boxes, st));
     DeviceBvh8 blas;
-    {
+    float4* prims = nullptr;
+    if (!flat) {
+        int* prim_mesh = nullptr;
+        float* boxes = nullptr;
+        if (int rc = X.get(&prim_mesh, T)) return rc;
+        if (int rc = X.get(&boxes, T * 6)) return rc;
+        LUX_CUDA(launch_fill_mesh_ids(d_tri_off, NM, prim_mesh, st));
+        LUX_CUDA(launch_tri_boxes(pos, idx, prim_mesh, d_vert_off, int(T), boxes, st));
         std::vector<int> tb(tri_off.begin(), tri_off.end());
         if (int rc = build_bvh8_device(boxes, tb, 0, false, st, blas)) return rc;
+        if (int rc = own(&prims, T * 3, sizeof(float4))) return rc;
+        LUX_CUDA(launch_tri_records(blas.leaf_prim, int(T), prim_mesh, d_tri_off, d_vert_off, pos, idx, prims, st));
     }
-    float4* prims = nullptr;
-    if (int rc = own(&prims, T * 3, sizeof(float4))) return rc;
-    LUX_CUDA(launch_tri_records(blas.leaf_prim, int(T), prim_mesh, d_tri_off, d_vert_off, pos, idx, prims, st));
-
     LUX_CUDA(cudaStreamSynchronize(st));
     G.ms_blas = ms_since(t0) - G.ms_upload;
     // ---- instances ----
@@ -185,7 +195,7 @@ int build_geometry(const lux_scene_desc* const* scenes, int ns, const std::vecto
             const lux_mesh_desc& md = *mesh[gm];
             I.mesh = in.mesh;
             I.material = in.material + material_base[s];
-            I.blas_root = blas.root[gm];
+            I.blas_root = flat ? 0u : blas.root[gm];
             I.prim_base = tri_off[gm];
             I.vert_base = vert_off[gm];
             I.idx_base = tri_off[gm];
@@ -195,7 +205,7 @@ int build_geometry(const lux_scene_desc* const* scenes, int ns, const std::vecto
             I.num_tris = md.num_tris;
             I.key = i;
             G.instanced_tris[s] += md.num_tris;
-            G.max_blas_depth[s] = std::max(G.max_blas_depth[s], blas.depth[gm]);
+            if (!flat) G.max_blas_depth[s] = std::max(G.max_blas_depth[s], blas.depth[gm]);
         }
     }
     DevInstance* d_insts = nullptr;
@@ -224,6 +234,56 @@ int build_geometry(const lux_scene_desc* const* scenes, int ns, const std::vecto
         const int i0 = G.inst_base[s], n = G.inst_base[s + 1] - i0;
         LUX_CUDA(launch_inst_boxes(d_M + size_t(i0) * 12, d_inst_mesh + i0, n, pos, d_vert_off, mesh_box, exact,
                                    ibox + size_t(i0) * 6, st));
+    }
+    if (flat) {
+        // ---- single-level layout: one world-space BVH per scene over its instanced triangles ----
+        std::vector<uint32_t> itri(size_t(NI) + 1, 0);
+        for (int i = 0; i < NI; ++i) itri[i + 1] = itri[i] + uint32_t(mesh[inst_mesh[i]]->num_tris);
+        const size_t NT = itri[NI];
+        uint32_t* d_itri = nullptr;
+        int* flat_inst = nullptr;
+        float* fbox = nullptr;
+        if (int rc = X.get(&d_itri, size_t(NI) + 1)) return rc;
+        if (int rc = X.get(&flat_inst, NT)) return rc;
+        if (int rc = X.get(&fbox, NT * 6)) return rc;
+        LUX_CUDA(cudaMemcpyAsync(d_itri, itri.data(), sizeof(uint32_t) * (NI + 1), cudaMemcpyHostToDevice, st));
+        LUX_CUDA(launch_fill_mesh_ids(d_itri, NI, flat_inst, st));
+        LUX_CUDA(launch_flat_boxes(d_M, d_inst_mesh, d_itri, flat_inst, int(NT), ibox, pos, idx, d_tri_off, d_vert_off,
+                                   fbox, st));
+        std::vector<int> tb(size_t(ns) + 1);
+        for (int s = 0; s <= ns; ++s) tb[s] = int(itri[G.inst_base[s]]);
+        DeviceBvh8 world;
+        if (int rc = build_bvh8_device(fbox, tb, 0, true, st, world)) return rc;
+        for (int s = 0; s < ns; ++s)
+            if (world.depth[s] + 4 > 16 + 48)
+                return fail(LUX_ERR_UNSUPPORTED, "acceleration structure deeper than the traversal stack");
+        BVH8Node* nodes = nullptr;
+        float4* fprims = nullptr;
+        if (int rc = own(&nodes, world.num_nodes, sizeof(BVH8Node))) return rc;
+        if (int rc = own(&fprims, NT * 3, sizeof(float4))) return rc;
+        LUX_CUDA(cudaMemcpyAsync(nodes, world.nodes, sizeof(BVH8Node) * world.num_nodes, cudaMemcpyDeviceToDevice, st));
+        LUX_CUDA(launch_flat_records(world.leaf_prim, int(NT), flat_inst, d_itri, d_inst_mesh, d_tri_off, d_vert_off, pos,
+                                     idx, fprims, st));
+        LUX_CUDA(cudaStreamSynchronize(st));
+        G.ms_total = ms_since(t0);
+        G.ms_tlas = G.ms_total - G.ms_upload - G.ms_blas;
+        S.nodes = reinterpret_cast<const uint4*>(nodes);
+        S.prims = fprims;
+        S.insts = d_insts;
+        S.tlas_prims = nullptr;
+        S.tlas_leaf = nullptr;
+        S.tlas_root = world.root[0];
+        S.num_insts = NI;
+        S.single_level = 1;
+        S.pos = pos;
+        S.nrm = nrm;
+        S.uv = uv;
+        S.idx = idx;
+        G.tlas_root = world.root;
+        G.blas_nodes = 0;
+        G.tlas_nodes = world.num_nodes;
+        G.single_level = true;
+        return LUX_OK;
     }
     DeviceBvh8 tlas;
     {
@@ -272,6 +332,7 @@ int build_geometry(const lux_scene_desc* const* scenes, int ns, const std::vecto
     S.tlas_leaf = tlas_leaf;
     S.tlas_root = tlas.root[0];
     S.num_insts = NI;
+    S.single_level = 0;
     S.pos = pos;
     S.nrm = nrm;
     S.uv = uv;
@@ -279,6 +340,7 @@ int build_geometry(const lux_scene_desc* const* scenes, int ns, const std::vecto
     G.tlas_root = tlas.root;
     G.blas_nodes = blas.num_nodes;
     G.tlas_nodes = tlas.num_nodes;
+    G.single_level = false;
     return LUX_OK;
 }
 

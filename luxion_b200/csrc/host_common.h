@@ -116,15 +116,17 @@ struct GeometryBuild {
     std::vector<int> max_blas_depth;      // per scene
     uint32_t blas_nodes = 0, tlas_nodes = 0;
     double ms_upload = 0, ms_blas = 0, ms_tlas = 0, ms_total = 0;  // host wall time per stage
+    bool single_level = false;
     size_t bytes = 0;                     // device bytes allocated through alloc
 };
 
-// Device geometry of ns scenes concatenated (geometry.cpp): vertex data, every mesh's BLAS and
-// every scene's TLAS built on the device, triangle records, instance records (materials
+// Device geometry of ns scenes concatenated (geometry.cpp): vertex data and, by layout
+// (LUX_BVH_*), either every mesh's BLAS and every scene's TLAS or one world-space BVH per scene
+// over its instanced triangles, built on the device, triangle records, instance records (materials
 // offset by material_base[s]) and TLAS leaf records. Fills S.nodes, prims, insts, tlas_prims,
 // tlas_leaf, tlas_root (scene 0), num_insts, pos, nrm, uv, idx. Runs on stream st and returns
 // once the build has finished.
-int build_geometry(const lux_scene_desc* const* scenes, int ns, const std::vector<int>& material_base,
+int build_geometry(const lux_scene_desc* const* scenes, int ns, const std::vector<int>& material_base, int layout,
                    const DevAlloc& alloc, cudaStream_t st, DevScene& S, GeometryBuild& G);
 
 // Check a scene description (sizes, index ranges, references, environment format).

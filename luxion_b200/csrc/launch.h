@@ -9,7 +9,8 @@ namespace lux {
 constexpr int kTraceBlock = 128;
 constexpr int kShadeBlock = 128;
 
-int trace_grid_blocks(int mode);
+// persistent traversal grid of `mode` for the two-level or the single-level layout
+int trace_grid_blocks(int mode, bool single = false);
 int shade_grid_blocks();
 
 // persistent trace of bounce `bounce`: mode 0 radiance (queues shadow rays when nee != 0:

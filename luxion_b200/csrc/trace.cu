@@ -149,21 +149,19 @@ LUX_DI bool better(float t, int inst, int prim, const Best& b) {
     return t == b.t && (inst < b.inst || (inst == b.inst && prim < b.prim));
 }
 
-// Moller-Trumbore exactly as src/intersections/mesh_isect.cu:78-115, single-rounded ops.
-LUX_DI bool mt_test(const float4* __restrict__ prims, uint32_t rec, const TRay& r, float& t, float& u, float& v,
-                    int& prim) {
-    const float4* q = prims + size_t(rec) * 3;
-    float4 a4 = __ldg(q), e14 = __ldg(q + 1), e24 = __ldg(q + 2);
+// Moller-Trumbore exactly as src/intersections/mesh_isect.cu:78-115, single-rounded ops, on a
+// triangle record (v0 with the triangle index in w, e1, e2) and the ray (ro, d) of the
+// triangle's object space.
+LUX_DI bool mt_core(float4 a4, float4 e14, float4 e24, f3 ro, f3 d, float& t, float& u, float& v, int& prim) {
     prim = __float_as_int(a4.w);
     const f3 e1 = mk(e14.x, e14.y, e14.z), e2 = mk(e24.x, e24.y, e24.z);
-    const f3 d = r.d;
     // cross(d, e2) = (d.y*e2.z - e2.y*d.z, d.z*e2.x - e2.z*d.x, d.x*e2.y - e2.x*d.y)
     f3 c = mk(__fsub_rn(__fmul_rn(d.y, e2.z), __fmul_rn(e2.y, d.z)), __fsub_rn(__fmul_rn(d.z, e2.x), __fmul_rn(e2.z, d.x)),
               __fsub_rn(__fmul_rn(d.x, e2.y), __fmul_rn(e2.x, d.y)));
     float det = __fadd_rn(__fadd_rn(__fmul_rn(e1.x, c.x), __fmul_rn(e1.y, c.y)), __fmul_rn(e1.z, c.z));
     if (det > -kMT_EPS && det < kMT_EPS) return false;
     float inv = __frcp_rn(det);
-    f3 a = mk(__fsub_rn(r.o.x, a4.x), __fsub_rn(r.o.y, a4.y), __fsub_rn(r.o.z, a4.z));
+    f3 a = mk(__fsub_rn(ro.x, a4.x), __fsub_rn(ro.y, a4.y), __fsub_rn(ro.z, a4.z));
     u = __fmul_rn(inv, __fadd_rn(__fadd_rn(__fmul_rn(a.x, c.x), __fmul_rn(a.y, c.y)), __fmul_rn(a.z, c.z)));
     if (u < -kMT_EPS || u > 1.0f + kMT_EPS) return false;
     // cross(a, e1)
@@ -174,6 +172,12 @@ LUX_DI bool mt_test(const float4* __restrict__ prims, uint32_t rec, const TRay& 
     if ((v < 0.0f && fabsf(v) > kMT_EPS) || (uv > 1.0f && fabsf(__fsub_rn(uv, 1.0f)) > kMT_EPS)) return false;
     t = __fmul_rn(inv, __fadd_rn(__fadd_rn(__fmul_rn(e2.x, c.x), __fmul_rn(e2.y, c.y)), __fmul_rn(e2.z, c.z)));
     return t > kMT_EPS;
+}
+
+LUX_DI bool mt_test(const float4* __restrict__ prims, uint32_t rec, const TRay& r, float& t, float& u, float& v,
+                    int& prim) {
+    const float4* q = prims + size_t(rec) * 3;
+    return mt_core(__ldg(q), __ldg(q + 1), __ldg(q + 2), r.o, r.d, t, u, v, prim);
 }
 
 // Any-hit program (src/optixshaders/optix_triangle.cu:317-366): true = accept the hit.
@@ -215,10 +219,12 @@ LUX_DI bool alpha_accept(const DevScene& S, const DevInstance& I, int inst, int 
     return !(rnd >= alpha);
 }
 
-// Traversal state of one lane. The world ray is kept as origin and direction only; its
-// reciprocals are recomputed when the traversal leaves an instance.
+// Traversal state of one lane. Two-level layout: wo, wd hold the world ray (its reciprocals are
+// recomputed when the traversal leaves an instance) and cur the ray of the current level.
+// Single-level layout: cur is the world ray throughout, and wo, wd hold the object-space ray of
+// the instance `inst` whose triangles were tested last.
 struct Lane {
-    f3 wo, wd;          // world ray
+    f3 wo, wd;          // world ray (two-level) / object ray of `inst` (single-level)
     TRay cur;           // ray of the current level (world in the TLAS, object space in a BLAS)
     float tmax;
     Best best;
@@ -234,7 +240,7 @@ struct Lane {
     bool done;
 };
 
-template <int MODE>
+template <int MODE, bool SINGLE>
 struct Tracer {
     const DevScene& S;
     uint2 (*sh)[kTraceBlock];  // shared stack [kShStack][block]
@@ -277,6 +283,8 @@ struct Tracer {
     }
 
     LUX_DI float limit(const Lane& L) const { return (MODE != 2 && L.best.inst >= 0) ? L.best.t : L.tmax; }
+    static LUX_DI f3 world_o(const Lane& L) { return SINGLE ? L.cur.o : L.wo; }
+    static LUX_DI f3 world_d(const Lane& L) { return SINGLE ? L.cur.d : L.wd; }
 
     // Node phase: visit the nearest remaining child of the node group.
     LUX_DI void visit(Lane& L) {
@@ -292,7 +300,8 @@ struct Tracer {
         if (MODE == 3) ++L.work;
         L.g = make_uint2(cbase, (nimask << 8) | nkeys);
         if (tmask) {
-            if (L.inst >= 0) L.t = make_uint2(L.inst_prim_base + tbase, kTagTri | (lmask << 8) | tmask);
+            if (SINGLE) L.t = make_uint2(tbase, kTagTri | (lmask << 8) | tmask);
+            else if (L.inst >= 0) L.t = make_uint2(L.inst_prim_base + tbase, kTagTri | (lmask << 8) | tmask);
             else L.t = make_uint2(tbase, kTagInst | (lmask << 8) | tmask);
         }
     }
@@ -308,11 +317,29 @@ struct Tracer {
         float t, u, v;
         int prim;
         if (MODE == 3) ++L.work;
-        if (!mt_test(S.prims, L.t.x + uint32_t(k), L.cur, t, u, v, prim)) return;
+        if (SINGLE) {
+            // the record names its instance; the object-space ray is rebuilt when it changes,
+            // exactly as entering the instance from a TLAS leaf builds it
+            const float4* q = S.prims + size_t(L.t.x + uint32_t(k)) * 3;
+            const float4 a4 = __ldg(q), e14 = __ldg(q + 1), e24 = __ldg(q + 2);
+            const int inst = __float_as_int(e14.w);
+            if (inst != L.inst) {
+                const DevInstance& I = S.insts[inst];
+                float Minv[12];
+                for (int j = 0; j < 12; ++j) Minv[j] = __ldg(&I.Minv[j]);
+                L.wo = xform(Minv, L.cur.o, 1.0f);
+                L.wd = xform(Minv, L.cur.d, 0.0f);
+                L.inst = inst;
+                L.inst_flags = __ldg(&I.flags);
+            }
+            if (!mt_core(a4, e14, e24, L.wo, L.wd, t, u, v, prim)) return;
+        } else {
+            if (!mt_test(S.prims, L.t.x + uint32_t(k), L.cur, t, u, v, prim)) return;
+        }
         if (!(t <= L.tmax)) return;
         if (MODE != 2 && !better(t, L.inst, prim, L.best)) return;
         if (L.inst_flags & kInstAnyHit) {
-            if (!alpha_accept(S, S.insts[L.inst], L.inst, prim, u, v, L.wd, L.pixel, L.iter)) return;
+            if (!alpha_accept(S, S.insts[L.inst], L.inst, prim, u, v, world_d(L), L.pixel, L.iter)) return;
         }
         L.best.t = t;
         L.best.inst = L.inst;
@@ -415,14 +442,14 @@ LUX_DI f3 hit_world_normal(const DevScene& S, int inst, int prim, float bu, floa
     return mk(__fmul_rn(w.x, il), __fmul_rn(w.y, il), __fmul_rn(w.z, il));
 }
 
-template <int MODE>
+template <int MODE, bool SINGLE>
 // The arguments stay in parameter space (__grid_constant__): the tracer reads the scene
 // through a reference to them, which would otherwise copy the struct to local memory.
 // Seven 128-thread blocks per SM (at most 73 registers) measured faster than six (80) and
 // eight (64, with spills).
 __global__ void __launch_bounds__(kTraceBlock, 7) k_trace(const __grid_constant__ TraceArgs A) {
     __shared__ uint2 stack[kShStack][kTraceBlock];
-    Tracer<MODE> T{A.S, stack, {}, int(threadIdx.x), &A.W.ctr->error};
+    Tracer<MODE, SINGLE> T{A.S, stack, {}, int(threadIdx.x), &A.W.ctr->error};
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const bool ext = A.ext_rays != nullptr;
@@ -543,7 +570,7 @@ __global__ void __launch_bounds__(kTraceBlock, 7) k_trace(const __grid_constant_
                     if (hit && A.nee) {
                         // shadow ray of the raygen program (src/optixshaders/optix_triangle.cu:82-132)
                         f3 n = hit_world_normal(A.S, L.best.inst, L.best.prim, L.best.u, L.best.v);
-                        f3 wo = L.wo, wd = L.wd;
+                        const f3 wo = Tracer<MODE, SINGLE>::world_o(L), wd = Tracer<MODE, SINGLE>::world_d(L);
                         f3 hp = mk(__fadd_rn(wo.x, __fmul_rn(L.best.t, wd.x)), __fadd_rn(wo.y, __fmul_rn(L.best.t, wd.y)),
                                    __fadd_rn(wo.z, __fmul_rn(L.best.t, wd.z)));
                         f3 so = mk(__fadd_rn(hp.x, __fmul_rn(n.x, 1e-4f)), __fadd_rn(hp.y, __fmul_rn(n.y, 1e-4f)),
@@ -598,43 +625,59 @@ __global__ void __launch_bounds__(kTraceBlock, 7) k_trace(const __grid_constant_
 // Persistent grid of each traversal kind: SMs x resident blocks per SM. The answer depends on
 // the device, so it is cached per device ordinal, under a lock (contexts on several devices and
 // several host threads ask for it).
-int trace_grid_blocks(int mode) {
+int trace_grid_blocks(int mode, bool single) {
     static std::mutex mu;
-    static std::map<int, std::array<int, 4>> cache;
+    static std::map<int, std::array<int, 8>> cache;
     int dev = 0;
     cudaGetDevice(&dev);
     std::lock_guard<std::mutex> lock(mu);
-    int& cached = cache[dev][mode];
+    int& cached = cache[dev][mode * 2 + (single ? 1 : 0)];
     if (cached == 0) {
         int sms = 0, per = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (mode == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace<0>, kTraceBlock, 0);
-        else if (mode == 1) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace<1>, kTraceBlock, 0);
-        else if (mode == 2) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace<2>, kTraceBlock, 0);
-        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace<3>, kTraceBlock, 0);
+        if (single) {
+            if (mode == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace<0, true>, kTraceBlock, 0);
+            else if (mode == 1) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace<1, true>, kTraceBlock, 0);
+            else if (mode == 2) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace<2, true>, kTraceBlock, 0);
+            else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace<3, true>, kTraceBlock, 0);
+        } else {
+            if (mode == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace<0, false>, kTraceBlock, 0);
+            else if (mode == 1) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace<1, false>, kTraceBlock, 0);
+            else if (mode == 2) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace<2, false>, kTraceBlock, 0);
+            else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trace<3, false>, kTraceBlock, 0);
+        }
         cached = sms * (per > 0 ? per : 1);
     }
     return cached;
 }
 
+namespace {
+template <bool SINGLE>
+void launch_mode(int mode, int grid, cudaStream_t st, const TraceArgs& A) {
+    if (mode == 0) k_trace<0, SINGLE><<<grid, kTraceBlock, 0, st>>>(A);
+    else if (mode == 1) k_trace<1, SINGLE><<<grid, kTraceBlock, 0, st>>>(A);
+    else if (mode == 2) k_trace<2, SINGLE><<<grid, kTraceBlock, 0, st>>>(A);
+    else k_trace<3, SINGLE><<<grid, kTraceBlock, 0, st>>>(A);
+}
+}  // namespace
+
 cudaError_t launch_trace(const DevScene& S, const DevWave& W, int bounce, int mode, int nee, cudaStream_t st,
                          int grid) {
     TraceArgs A{S, W, bounce, mode, nee, nullptr, nullptr, 0, 0, nullptr};
-    if (grid <= 0) grid = trace_grid_blocks(mode);
-    if (mode == 0) k_trace<0><<<grid, kTraceBlock, 0, st>>>(A);
-    else if (mode == 1) k_trace<1><<<grid, kTraceBlock, 0, st>>>(A);
-    else if (mode == 2) k_trace<2><<<grid, kTraceBlock, 0, st>>>(A);
-    else k_trace<3><<<grid, kTraceBlock, 0, st>>>(A);
+    const bool single = S.single_level != 0;
+    if (grid <= 0) grid = trace_grid_blocks(mode, single);
+    if (single) launch_mode<true>(mode, grid, st, A);
+    else launch_mode<false>(mode, grid, st, A);
     return cudaGetLastError();
 }
 
 cudaError_t launch_trace_ext(const DevScene& S, const DevWave& W, const float* rays, uint32_t* hits, int n, int mode,
                              int iter, int* fetch, cudaStream_t st) {
     TraceArgs A{S, W, 0, mode, 0, rays, hits, n, iter, fetch};
-    int grid = trace_grid_blocks(mode);
-    if (mode == 0) k_trace<0><<<grid, kTraceBlock, 0, st>>>(A);
-    else if (mode == 1) k_trace<1><<<grid, kTraceBlock, 0, st>>>(A);
-    else k_trace<2><<<grid, kTraceBlock, 0, st>>>(A);
+    const bool single = S.single_level != 0;
+    const int grid = trace_grid_blocks(mode, single);
+    if (single) launch_mode<true>(mode, grid, st, A);
+    else launch_mode<false>(mode, grid, st, A);
     return cudaGetLastError();
 }
 

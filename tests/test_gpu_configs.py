@@ -15,6 +15,7 @@ import pytest
 
 import luxion_b200 as lx
 import oracle_lib as ol
+from luxion_b200 import _ffi
 from luxion_b200._ffi import default_options
 
 pytestmark = pytest.mark.gpu
@@ -53,11 +54,11 @@ def test_c1_full_image_parity():
         assert frac >= PIXEL_FRAC and relmse <= RELMSE_TOL, ("reference crop", frac, relmse)
 
 
-@pytest.fixture(scope="module")
-def c2():
+@pytest.fixture(scope="module", params=[_ffi.BVH_SINGLE_LEVEL, _ffi.BVH_TWO_LEVEL], ids=["single", "two_level"])
+def c2(request):
     s = lx.random_scene(seed=0)
     assert s.instanced_tris > 990000 and s.desc.num_instances == 200
-    opt = default_options(direct_light_sampling=1, env_importance_sampling=1)
+    opt = default_options(direct_light_sampling=1, env_importance_sampling=1, bvh_layout=request.param)
     r = lx.Renderer(s, opt)
     o = ol.OracleScene(s)
     W, H = s.width, s.height

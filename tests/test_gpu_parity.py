@@ -45,11 +45,13 @@ def small_random_scene(**kw):
 OPTS = {"cornell": dict(direct_light_sampling=1), "rand": dict(direct_light_sampling=1, env_importance_sampling=1)}
 
 
-@pytest.fixture(scope="module", params=["cornell", "rand"])
+@pytest.fixture(scope="module", params=["cornell", "rand", "rand_two_level"])
 def pair(request):
     tag = request.param
+    layout = _ffi.BVH_TWO_LEVEL if tag.endswith("two_level") else _ffi.BVH_AUTO
+    tag = tag.replace("_two_level", "")
     s = lx.cornell36(48, 48) if tag == "cornell" else small_random_scene()
-    r = lx.Renderer(s, default_options(**OPTS[tag]))
+    r = lx.Renderer(s, default_options(**OPTS[tag], bvh_layout=layout))
     yield tag, s, r, ol.OracleScene(s), default_options(**OPTS[tag])
     r.close()
 
@@ -111,12 +113,14 @@ def test_trace_hits_bit_exact_golden(g, pair):
     assert np.array_equal(r.trace_rays(g[f"{tag}_rand_rays_tmax"], 1, 3), g[f"{tag}_trace_rand_m1"])
 
 
-@pytest.fixture(scope="module")
-def mid_scene():
+# Both BVH layouts (one world-space BVH over instanced triangles; per-mesh BLASes under a TLAS)
+# must give the same hits bit for bit: every triangle is tested in its instance's object space.
+@pytest.fixture(scope="module", params=[_ffi.BVH_SINGLE_LEVEL, _ffi.BVH_TWO_LEVEL], ids=["single", "two_level"])
+def mid_scene(request):
     s = lx.random_scene(seed=21, num_instances=40, total_tris=200000, min_tris=2000, max_tris=20000,
                         num_emissive=4, num_textures=4, texture_size=64, env_width=64, env_height=32,
                         width=64, height=36, trace_depth=8)
-    r = lx.Renderer(s, default_options(direct_light_sampling=1, env_importance_sampling=1))
+    r = lx.Renderer(s, default_options(direct_light_sampling=1, env_importance_sampling=1, bvh_layout=request.param))
     yield s, r, ol.OracleScene(s)
     r.close()
 
