@@ -591,17 +591,24 @@ def main():
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             rr = lx.Renderer(scene, opt)
+            t_init = time.perf_counter()
             rr.render(1 + rank * SPP, SPP)
             img_host[...] = rr.image_sum()
+            t_copy = time.perf_counter()
             st = rr.stats()
+            stages = rr.scene_stats()
             rr.close()
             torch.cuda.synchronize()
             e_ms.append((time.perf_counter() - t0) * 1e3)
+            if e_ms[-1] == min(e_ms):
+                split = {"lux_init_ms": (t_init - t0) * 1e3, "render_and_copy_ms": (t_copy - t_init) * 1e3,
+                         "lux_free_ms": (time.perf_counter() - t_copy) * 1e3,
+                         "scene_build_stages_ms": {k: round(v, 2) for k, v in stages.items() if k.startswith("ms_")}}
             e_rays = st["rays_radiance"] + st["rays_shadow"]
         h2d = scene_bytes(scene)
         e2e = {"value": e_rays / (min(e_ms) * 1e-3) / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(W * H * 12), "ms_per_step": min(e_ms), "ms_runs": e_ms,
-               "host_memory": "page-locked" if pinned else "pageable",
+               "host_memory": "page-locked" if pinned else "pageable", "split": split,
                "includes": "lux_init (scene upload, device BVH8 build, light tables, textures), "
                            "lux_render 16 spp, lux_copy_image, lux_free"}
         # the drop-in's own cycle on a resident scene: pathtraceInit (lux_init_on_scene),

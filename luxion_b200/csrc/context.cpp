@@ -75,19 +75,25 @@ struct lux_scene {
     lux_scene_stats stats{};     // stage times of the build
     std::atomic<int> refs{1};
 
+    // Device memory of the scene: stream-ordered from the library's pool on the scene's own
+    // stream (the geometry is built on it), so building and freeing a scene never waits for
+    // the whole device; host tables are copied on the same stream.
+    cudaStream_t stream = nullptr;
     template <class T>
     int alloc(T** p, size_t n) {
-        int rc = dalloc(p, n);
-        if (rc == LUX_OK && *p) allocs.push_back(*p);
+        *p = nullptr;
+        if (n == 0) return LUX_OK;
+        cudaError_t e = scratch_alloc(reinterpret_cast<void**>(p), n * sizeof(T), stream);
+        if (e != cudaSuccess) return fail(LUX_ERR_OOM, std::string("device allocation: ") + cudaGetErrorString(e));
+        allocs.push_back(*p);
         scene_bytes += n * sizeof(T);
-        return rc;
+        return LUX_OK;
     }
     template <class T>
     int up(T** p, const T* src, size_t n) {
-        int rc = upload(p, src, n);
-        if (rc == LUX_OK && *p) allocs.push_back(*p);
-        scene_bytes += n * sizeof(T);
-        return rc;
+        if (int rc = alloc(p, n)) return rc;
+        if (n) LUX_CUDA(cudaMemcpyAsync(*p, src, n * sizeof(T), cudaMemcpyHostToDevice, stream));
+        return LUX_OK;
     }
 };
 
@@ -149,33 +155,40 @@ float half_bits_to_float(uint16_t h) {
 // device, texconv.cu),
 // LUX_TEXSTORE_HALF converts them to binary16, LUX_TEXSTORE_UNORM8 keeps 8-bit texels (16-bit
 // ones become float4). Binary16 texels stay binary16 under every storage.
-// Device staging for texel conversion, reused across the textures of one scene build.
+// The texture uploads of one scene build run asynchronously on one stream: host texels are
+// copied to device staging (pool memory, freed once the stream has drained), converted there,
+// and copied into their CUDA arrays; one synchronisation ends the batch.
 struct TexStage {
-    void* src = nullptr;
-    void* dst = nullptr;
-    size_t src_bytes = 0, dst_bytes = 0;
+    cudaStream_t st = nullptr;
+    std::vector<void*> staging;
     TexStage() = default;
     TexStage(const TexStage&) = delete;
     TexStage& operator=(const TexStage&) = delete;
-    ~TexStage() {
-        if (src) cudaFree(src);
-        if (dst) cudaFree(dst);
+    int begin() {
+        LUX_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        return LUX_OK;
     }
-    int reserve(size_t sb, size_t db) {
-        if (sb > src_bytes) {
-            if (src) cudaFree(src);
-            src = nullptr;
-            src_bytes = 0;
-            LUX_CUDA(cudaMalloc(&src, sb));
-            src_bytes = sb;
+    int finish() {
+        if (!st) return LUX_OK;
+        cudaError_t e = cudaStreamSynchronize(st);
+        release();
+        if (e != cudaSuccess) return fail(LUX_ERR_CUDA, std::string("texture upload: ") + cudaGetErrorString(e));
+        return LUX_OK;
+    }
+    void release() {
+        for (void* p : staging) scratch_free(p, st);
+        staging.clear();
+        if (st) {
+            cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
         }
-        if (db > dst_bytes) {
-            if (dst) cudaFree(dst);
-            dst = nullptr;
-            dst_bytes = 0;
-            LUX_CUDA(cudaMalloc(&dst, db));
-            dst_bytes = db;
-        }
+        st = nullptr;
+    }
+    ~TexStage() { release(); }
+    int get(void** p, size_t bytes) {
+        cudaError_t e = scratch_alloc(p, bytes, st);
+        if (e != cudaSuccess) return fail(LUX_ERR_OOM, std::string("texture staging: ") + cudaGetErrorString(e));
+        staging.push_back(*p);
         return LUX_OK;
     }
 };
@@ -192,10 +205,12 @@ int make_texture(const lux_texture_desc& t, DevTex& out, int storage, TexStage& 
     const void* dev_src = nullptr;
     if (to_half || to_float) {
         const size_t in_bytes = t.format == LUX_TEX_RGBA8 ? 1 : (t.format == LUX_TEX_RGBA32F ? 4 : 2);
-        if (int rc = stage.reserve(n * in_bytes, n * (to_half ? 2 : 4))) return rc;
-        LUX_CUDA(cudaMemcpy(stage.src, t.data, n * in_bytes, cudaMemcpyHostToDevice));
-        LUX_CUDA(launch_convert_texels(stage.src, t.format, to_half ? 1 : 0, stage.dst, n, 0));
-        dev_src = stage.dst;
+        void *s_in = nullptr, *s_out = nullptr;
+        if (int rc = stage.get(&s_in, n * in_bytes)) return rc;
+        if (int rc = stage.get(&s_out, n * (to_half ? 2 : 4))) return rc;
+        LUX_CUDA(cudaMemcpyAsync(s_in, t.data, n * in_bytes, cudaMemcpyHostToDevice, stage.st));
+        LUX_CUDA(launch_convert_texels(s_in, t.format, to_half ? 1 : 0, s_out, n, stage.st));
+        dev_src = s_out;
         fmt = to_half ? LUX_TEX_RGBA16F : LUX_TEX_RGBA32F;
     }
     cudaChannelFormatDesc fd;
@@ -225,11 +240,11 @@ int make_texture(const lux_texture_desc& t, DevTex& out, int storage, TexStage& 
     }
     LUX_CUDA(cudaMallocArray(&out.arr, &fd, t.width, t.height));
     if (dev_src)
-        LUX_CUDA(cudaMemcpy2DToArray(out.arr, 0, 0, dev_src, size_t(t.width) * texel, size_t(t.width) * texel,
-                                     t.height, cudaMemcpyDeviceToDevice));
+        LUX_CUDA(cudaMemcpy2DToArrayAsync(out.arr, 0, 0, dev_src, size_t(t.width) * texel, size_t(t.width) * texel,
+                                          t.height, cudaMemcpyDeviceToDevice, stage.st));
     else
-        LUX_CUDA(cudaMemcpy2DToArray(out.arr, 0, 0, src, size_t(t.width) * texel, size_t(t.width) * texel, t.height,
-                                     cudaMemcpyHostToDevice));
+        LUX_CUDA(cudaMemcpy2DToArrayAsync(out.arr, 0, 0, src, size_t(t.width) * texel, size_t(t.width) * texel,
+                                          t.height, cudaMemcpyHostToDevice, stage.st));
     out.bytes = size_t(t.width) * t.height * texel;
     cudaResourceDesc rd{};
     rd.resType = cudaResourceTypeArray;
@@ -408,6 +423,7 @@ int lux::build_host_scene(const lux_scene_desc& d, const lux_options& opt, std::
         }
         {
             TexStage stage;
+            tex_rc = stage.begin();
             for (int t = 0; t < d.num_textures && tex_rc == LUX_OK; ++t)
                 tex_rc = make_texture(d.textures[t], texs[tex0 + t], opt.texture_storage, stage);
             if (tex_rc == LUX_OK && d.env_data) {
@@ -415,6 +431,8 @@ int lux::build_host_scene(const lux_scene_desc& d, const lux_options& opt, std::
                 tex_rc = make_texture(et, env, opt.texture_storage == LUX_TEXSTORE_HALF ? LUX_TEXSTORE_HALF : LUX_TEXSTORE_FLOAT,
                                       stage);
             }
+            const int frc = stage.finish();
+            if (tex_rc == LUX_OK) tex_rc = frc;
         }
         H.ms_textures = ms_since(t0);
         if (tex_rc == LUX_OK && device_work) tex_rc = device_work();
@@ -545,8 +563,7 @@ int build_scene(lux_scene* R, const lux_scene_desc& d, const lux_options& opt, c
     int geo_rc = LUX_OK;
     std::string geo_err;
     std::thread geom([&]() {
-        cudaStream_t st = nullptr;
-        if (cudaSetDevice(dev) != cudaSuccess || cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+        if (cudaSetDevice(dev) != cudaSuccess) {
             geo_rc = fail(LUX_ERR_CUDA, "geometry thread set-up failed");
             geo_err = g_err;
             return;
@@ -554,9 +571,8 @@ int build_scene(lux_scene* R, const lux_scene_desc& d, const lux_options& opt, c
         const lux_scene_desc* one = &d;
         geo_rc = build_geometry(&one, 1, std::vector<int>{0}, opt.bvh_layout,
                                 [&](void** p, size_t bytes) { return R->alloc(reinterpret_cast<char**>(p), bytes); },
-                                st, geo, G);
+                                R->stream, geo, G);
         if (geo_rc) geo_err = g_err;
-        cudaStreamDestroy(st);
     });
     HostScene H;
     int rc = build_host_scene(d, opt, R->texs, R->env, H, device_work);
@@ -584,6 +600,7 @@ int build_scene(lux_scene* R, const lux_scene_desc& d, const lux_options& opt, c
     R->S = geo;
     if ((rc = upload_scene_materials(R, H, R->S))) return rc;
     if ((rc = upload_scene_lights(R, H, R->S))) return rc;
+    LUX_CUDA(cudaStreamSynchronize(R->stream));
     st.ms_total = ms_since(t_start);
     st.device_bytes = int64_t(R->scene_bytes);
     return LUX_OK;
@@ -594,7 +611,11 @@ void scene_release(lux_scene* R) {
     cudaSetDevice(R->device);
     for (auto& t : R->texs) destroy_texture(t);
     destroy_texture(R->env);
-    for (void* p : R->allocs) cudaFree(p);
+    for (void* p : R->allocs) scratch_free(p, R->stream);
+    if (R->stream) {
+        cudaStreamSynchronize(R->stream);
+        cudaStreamDestroy(R->stream);
+    }
     delete R;
 }
 
@@ -623,6 +644,10 @@ int scene_create(const lux_scene_desc& d, const lux_options& o, const std::funct
     *out = nullptr;
     lux_scene* R = new lux_scene();
     R->device = o.device;
+    if (cudaStreamCreateWithFlags(&R->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete R;
+        return fail(LUX_ERR_CUDA, "cudaStreamCreate failed");
+    }
     R->precision = o.precision;
     R->texture_storage = o.texture_storage;
     R->trace_depth = d.trace_depth;
