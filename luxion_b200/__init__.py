@@ -287,6 +287,13 @@ class Renderer:
         _check(lib().lux_copy_image(self._h, ptr(out)))
         return out
 
+    def image_sum_into(self, out: np.ndarray) -> np.ndarray:
+        """The accumulation sum into a caller's float32 (height, width, 3) array."""
+        if out.dtype != np.float32 or out.shape != (self.height, self.width, 3) or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float32 array of shape (height, width, 3)")
+        _check(lib().lux_copy_image(self._h, ptr(out)))
+        return out
+
     def rgba8(self) -> np.ndarray:
         out = np.empty((self.height, self.width, 4), np.uint8)
         _check(lib().lux_copy_rgba8(self._h, out.ctypes.data_as(C.POINTER(C.c_uint8))))

@@ -16,6 +16,8 @@
 #include <cfloat>
 #include <cmath>
 #include <cstring>
+#include <mutex>
+#include <thread>
 
 namespace lux {
 
@@ -45,6 +47,38 @@ bool invert4(const float* m, double* out) {
     for (int r = 0; r < 4; ++r)
         for (int c = 0; c < 4; ++c) out[c * 4 + r] = t[r][c + 4];
     return true;
+}
+
+// Page-locked staging of the vertex uploads, kept for the process and grown on demand: the
+// caller's arrays (pageable or not) are gathered into it by host threads, so the upload is a
+// few large DMA copies instead of one small copy per mesh array. One build uses it at a time.
+constexpr size_t kStageLimit = size_t(2) << 30;
+struct PinnedStage {
+    std::mutex mu;
+    void* p = nullptr;
+    size_t cap = 0;
+    cudaError_t reserve(size_t bytes) {
+        if (bytes <= cap) return cudaSuccess;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        const size_t want = bytes + bytes / 4;
+        cudaError_t e = cudaHostAlloc(&p, want, cudaHostAllocDefault);
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+};
+PinnedStage g_stage;
+
+// Run fn(lo, hi) over [0, n) split into contiguous ranges, one per host thread.
+template <class F>
+void parallel_ranges(int n, F fn) {
+    unsigned nt = std::max(1u, std::min(std::thread::hardware_concurrency(), 32u));
+    nt = std::max(1u, std::min(nt, unsigned(n)));
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < nt; ++t) th.emplace_back(fn, int(int64_t(n) * t / nt), int(int64_t(n) * (t + 1) / nt));
+    fn(0, int(int64_t(n) / nt));
+    for (auto& t : th) t.join();
 }
 
 // Scratch device memory of one geometry build (stream-ordered, from the build pool).
@@ -109,7 +143,8 @@ int build_geometry(const lux_scene_desc* const* scenes, int ns, const std::vecto
         return alloc(reinterpret_cast<void**>(p), n * elem);
     };
 
-    // ---- vertex data: each mesh's arrays straight into its place ----
+    // ---- vertex data: gathered into page-locked staging by host threads, then four DMA
+    // copies (one per array); above the staging limit each mesh's arrays are copied directly ----
     float *pos = nullptr, *nrm = nullptr, *uv = nullptr;
     uint32_t* idx = nullptr;
     if (int rc = own(&pos, V * 3, sizeof(float))) return rc;
@@ -118,22 +153,50 @@ int build_geometry(const lux_scene_desc* const* scenes, int ns, const std::vecto
     if (any_uv)
         if (int rc = own(&uv, V * 2, sizeof(float))) return rc;
     if (int rc = own(&idx, T * 3, sizeof(uint32_t))) return rc;
-    for (int m = 0; m < NM; ++m) {
-        const lux_mesh_desc& md = *mesh[m];
-        const size_t nv = size_t(md.num_verts), nt = size_t(md.num_tris);
-        LUX_CUDA(cudaMemcpyAsync(pos + size_t(vert_off[m]) * 3, md.positions, nv * 12, cudaMemcpyHostToDevice, st));
-        LUX_CUDA(cudaMemcpyAsync(idx + size_t(tri_off[m]) * 3, md.indices, nt * 12, cudaMemcpyHostToDevice, st));
-        if (nrm) {
-            if (md.normals) LUX_CUDA(cudaMemcpyAsync(nrm + size_t(vert_off[m]) * 3, md.normals, nv * 12, cudaMemcpyHostToDevice, st));
-            else LUX_CUDA(cudaMemsetAsync(nrm + size_t(vert_off[m]) * 3, 0, nv * 12, st));
-        }
-        if (uv) {
-            if (md.uvs) LUX_CUDA(cudaMemcpyAsync(uv + size_t(vert_off[m]) * 2, md.uvs, nv * 8, cudaMemcpyHostToDevice, st));
-            else LUX_CUDA(cudaMemsetAsync(uv + size_t(vert_off[m]) * 2, 0, nv * 8, st));
+    const size_t b_pos = V * 12, b_nrm = nrm ? V * 12 : 0, b_uv = uv ? V * 8 : 0, b_idx = T * 12;
+    const size_t total = b_pos + b_nrm + b_uv + b_idx;
+    std::unique_lock<std::mutex> stage_lock(g_stage.mu);
+    if (total <= kStageLimit && g_stage.reserve(total) == cudaSuccess) {
+        char* h = static_cast<char*>(g_stage.p);
+        char *h_pos = h, *h_nrm = h + b_pos, *h_uv = h_nrm + b_nrm, *h_idx = h_uv + b_uv;
+        parallel_ranges(NM, [&](int m0, int m1) {
+            for (int m = m0; m < m1; ++m) {
+                const lux_mesh_desc& md = *mesh[m];
+                const size_t nv = size_t(md.num_verts), nt = size_t(md.num_tris);
+                std::memcpy(h_pos + size_t(vert_off[m]) * 12, md.positions, nv * 12);
+                std::memcpy(h_idx + size_t(tri_off[m]) * 12, md.indices, nt * 12);
+                if (nrm) {
+                    if (md.normals) std::memcpy(h_nrm + size_t(vert_off[m]) * 12, md.normals, nv * 12);
+                    else std::memset(h_nrm + size_t(vert_off[m]) * 12, 0, nv * 12);
+                }
+                if (uv) {
+                    if (md.uvs) std::memcpy(h_uv + size_t(vert_off[m]) * 8, md.uvs, nv * 8);
+                    else std::memset(h_uv + size_t(vert_off[m]) * 8, 0, nv * 8);
+                }
+            }
+        });
+        LUX_CUDA(cudaMemcpyAsync(pos, h_pos, b_pos, cudaMemcpyHostToDevice, st));
+        if (nrm) LUX_CUDA(cudaMemcpyAsync(nrm, h_nrm, b_nrm, cudaMemcpyHostToDevice, st));
+        if (uv) LUX_CUDA(cudaMemcpyAsync(uv, h_uv, b_uv, cudaMemcpyHostToDevice, st));
+        LUX_CUDA(cudaMemcpyAsync(idx, h_idx, b_idx, cudaMemcpyHostToDevice, st));
+    } else {
+        for (int m = 0; m < NM; ++m) {
+            const lux_mesh_desc& md = *mesh[m];
+            const size_t nv = size_t(md.num_verts), nt = size_t(md.num_tris);
+            LUX_CUDA(cudaMemcpyAsync(pos + size_t(vert_off[m]) * 3, md.positions, nv * 12, cudaMemcpyHostToDevice, st));
+            LUX_CUDA(cudaMemcpyAsync(idx + size_t(tri_off[m]) * 3, md.indices, nt * 12, cudaMemcpyHostToDevice, st));
+            if (nrm) {
+                if (md.normals) LUX_CUDA(cudaMemcpyAsync(nrm + size_t(vert_off[m]) * 3, md.normals, nv * 12, cudaMemcpyHostToDevice, st));
+                else LUX_CUDA(cudaMemsetAsync(nrm + size_t(vert_off[m]) * 3, 0, nv * 12, st));
+            }
+            if (uv) {
+                if (md.uvs) LUX_CUDA(cudaMemcpyAsync(uv + size_t(vert_off[m]) * 2, md.uvs, nv * 8, cudaMemcpyHostToDevice, st));
+                else LUX_CUDA(cudaMemsetAsync(uv + size_t(vert_off[m]) * 2, 0, nv * 8, st));
+            }
         }
     }
-
     LUX_CUDA(cudaStreamSynchronize(st));
+    stage_lock.unlock();
     G.ms_upload = ms_since(t0);
     // ---- BLAS of every mesh (two-level layout) ----
     Scratch X(st);
