@@ -318,8 +318,9 @@ int lux_trace_rays(lux_ctx* ctx, const float* rays, int n, int mode, int iter, u
  * the per-call cudaFree of lux_trace_rays stalls (cudaFree waits for the whole device).
  * Rays and hits are staged through one fixed array of 256 + 52 * LUX_TRACE_STATIC_MAX_RAYS
  * bytes (about 3.25 MiB) compiled into the library, one copy per device. Its address is
- * looked up (cudaGetSymbolAddress) on the first call made on each device, so make that first
- * call before any stream capture begins on that device.
+ * looked up (cudaGetSymbolAddress) on every call; the first call on a device may load the
+ * library's device code there, so make that first call before any stream capture begins on
+ * that device.
  * Must start at zero: the traversal's work cursor in that array and the context's traversal
  * error word; the call clears both on the context's stream before its launch. Nothing else
  * carries over from one call to the next.
@@ -327,6 +328,11 @@ int lux_trace_rays(lux_ctx* ctx, const float* rays, int n, int mode, int iter, u
  * the array and race: the library does not lock it, so serialise such calls. */
 #define LUX_TRACE_STATIC_MAX_RAYS 65536
 int lux_trace_rays_static(lux_ctx* ctx, const float* rays, int n, int mode, int iter, uint32_t* hits);
+
+/* Device allocations the library has made since it was loaded, on all devices: cudaMalloc,
+ * stream-ordered and pool allocations, CUDA arrays. A diagnostics hook with no counterpart in
+ * the reference; the tests use it to show that lux_trace_rays_static allocates nothing. */
+int64_t lux_device_alloc_count(void);
 
 /* BVH8 build parity (no counterpart in the reference; its builder is fill_bvh,
  * src/mesh/bvh_build.cu:15-318): build the compressed 8-wide BVH over n = tree_begin[num_trees]

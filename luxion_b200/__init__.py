@@ -54,6 +54,7 @@ SIGNATURES = {
     "lux_copy_image_device": (C.c_int, [_P, C.c_void_p]),
     "lux_trace_rays": (C.c_int, [_P, c_float_p, C.c_int, C.c_int, C.c_int, c_u32_p]),
     "lux_trace_rays_static": (C.c_int, [_P, c_float_p, C.c_int, C.c_int, C.c_int, c_u32_p]),
+    "lux_device_alloc_count": (C.c_int64, []),
     "lux_morton_keys": (C.c_int, [_P, c_float_p, C.c_int, c_u32_p]),
     "lux_bvh8_build": (C.c_int, [c_float_p, c_int_p, C.c_int, C.c_int, C.c_void_p, C.c_int, c_u32_p, c_u32_p, c_int_p,
                                  c_int_p]),
@@ -240,9 +241,10 @@ class ResidentScene:
         return {n: getattr(st, n) for n, _ in _ffi.SceneStats._fields_}
 
     def compatible(self, opt: Options) -> bool:
-        """Whether a context with these options can render on this build."""
-        return (opt.device, opt.precision, opt.texture_storage) == (
-            self.options.device, self.options.precision, self.options.texture_storage)
+        """Whether a context with these options can render on this build (the options that
+        shape a build are the same)."""
+        keys = ("device", "precision", "texture_storage", "bvh_layout")
+        return all(getattr(opt, k) == getattr(self.options, k) for k in keys)
 
     def close(self):
         if getattr(self, "_h", None):

@@ -57,7 +57,9 @@ cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t st) {
             pool = it->second;
         }
     }
-    return cudaMallocFromPoolAsync(p, bytes, pool, st);
+    cudaError_t r = cudaMallocFromPoolAsync(p, bytes, pool, st);
+    if (r == cudaSuccess) note_device_alloc();
+    return r;
 }
 
 void scratch_free(void* p, cudaStream_t st) {

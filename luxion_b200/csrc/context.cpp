@@ -239,6 +239,7 @@ int make_texture(const lux_texture_desc& t, DevTex& out, int storage, TexStage& 
             return fail(LUX_ERR_INVALID, "unknown texture format");
     }
     LUX_CUDA(cudaMallocArray(&out.arr, &fd, t.width, t.height));
+    note_device_alloc();
     if (dev_src)
         LUX_CUDA(cudaMemcpy2DToArrayAsync(out.arr, 0, 0, dev_src, size_t(t.width) * texel, size_t(t.width) * texel,
                                           t.height, cudaMemcpyDeviceToDevice, stage.st));
@@ -858,6 +859,7 @@ struct Tmp {
     T* get(size_t n) {
         void* q = nullptr;
         if (cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) return nullptr;
+        note_device_alloc();
         p.push_back(q);
         return static_cast<T*>(q);
     }
@@ -890,7 +892,15 @@ int lux::validate_scene_desc(const lux_scene_desc& d) {
     return LUX_OK;
 }
 
+namespace {
+std::atomic<int64_t> g_device_allocs{0};
+}
+
+void lux::note_device_alloc() { g_device_allocs.fetch_add(1, std::memory_order_relaxed); }
+
 extern "C" {
+
+int64_t lux_device_alloc_count(void) { return g_device_allocs.load(std::memory_order_relaxed); }
 
 void lux_default_options(lux_options* o) {
     if (!o) return;

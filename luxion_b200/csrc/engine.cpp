@@ -160,9 +160,11 @@ int admit(lux_engine* E) {
         if (E->cfg.hbm_budget_bytes > 0 && E->device_bytes() + int64_t(j.bytes) > E->cfg.hbm_budget_bytes) break;
         const size_t n = size_t(j.npix) * 3;
         LUX_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&j.image), n * sizeof(float), E->stream));
+        note_device_alloc();
         LUX_CUDA(cudaMemsetAsync(j.image, 0, n * sizeof(float), E->stream));
         if (E->opt.precision == LUX_PRECISION_COMPENSATED) {
             LUX_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&j.comp), n * sizeof(float), E->stream));
+            note_device_alloc();
             LUX_CUDA(cudaMemsetAsync(j.comp, 0, n * sizeof(float), E->stream));
         }
         j.slot = E->free_slots.back();

@@ -36,12 +36,16 @@ inline double ms_since(std::chrono::steady_clock::time_point t0) {
         }                                                                                   \
     } while (0)
 
+// Counts every device allocation the library makes (lux_device_alloc_count).
+void note_device_alloc();
+
 template <class T>
 int dalloc(T** p, size_t n) {
     *p = nullptr;
     if (n == 0) return LUX_OK;
     cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(T));
     if (e != cudaSuccess) return fail(LUX_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    note_device_alloc();
     return LUX_OK;
 }
 template <class T>

@@ -4,11 +4,11 @@
 // (rays, hits, the work cursor of the persistent traversal). lux_trace_rays_static stages them
 // through this one array instead, compiled into the library, so the call allocates nothing.
 // Each device holds its own copy of the array; its address is looked up with
-// cudaGetSymbolAddress the first time the call is made on that device, with that device current.
+// cudaGetSymbolAddress on every call, with that device current, so a device reset (which
+// reloads the module at another address) leaves no stale pointer behind.
 #include <cuda_runtime.h>
 
 #include <cstdint>
-#include <mutex>
 
 #include "luxion.h"
 #include "launch.h"
@@ -23,30 +23,18 @@ static_assert(kRayBytes % 256 == 0, "hit region starts 256-byte aligned");
 
 static __device__ __align__(256) unsigned char g_trace_scratch[kHeaderBytes + kRayBytes + kHitBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-void* g_base[kMaxDevices] = {};
-
 }  // namespace
 
 size_t trace_static_scratch_bytes() { return kHeaderBytes + kRayBytes + kHitBytes; }
 
 cudaError_t trace_static_scratch(int device, TraceScratch& out) {
-    if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+    int cur = -1;
+    cudaError_t e = cudaGetDevice(&cur);
+    if (e != cudaSuccess) return e;
+    if (cur != device) return cudaErrorInvalidDevice;
     void* base = nullptr;
-    {
-        std::lock_guard<std::mutex> lk(g_mu);
-        base = g_base[device];
-        if (!base) {
-            int cur = -1;
-            cudaError_t e = cudaGetDevice(&cur);
-            if (e != cudaSuccess) return e;
-            if (cur != device) return cudaErrorInvalidDevice;
-            e = cudaGetSymbolAddress(&base, g_trace_scratch);
-            if (e != cudaSuccess) return e;
-            g_base[device] = base;
-        }
-    }
+    e = cudaGetSymbolAddress(&base, g_trace_scratch);
+    if (e != cudaSuccess) return e;
     unsigned char* b = static_cast<unsigned char*>(base);
     out.cursor = reinterpret_cast<int*>(b);
     out.rays = reinterpret_cast<float*>(b + kHeaderBytes);

@@ -57,3 +57,18 @@ def test_largest_batch_and_limits(renderer):
     # the rejected call did no device work: the next call still matches
     small = _rays(1000, 9, 2)
     assert np.array_equal(renderer.trace_rays_static(small, 2, 6), renderer.trace_rays(small, 2, 6))
+
+
+def test_static_call_allocates_no_device_memory(renderer):
+    """The entry point's defining property: lux_trace_rays_static makes no device allocation
+    (lux_device_alloc_count is unchanged across it), while lux_trace_rays makes its per-call
+    temporaries."""
+    rays = _rays(30000, 11, 0)
+    renderer.trace_rays_static(rays, 0, 3)   # the device code and scratch are loaded
+    count = lx.lib().lux_device_alloc_count
+    before = count()
+    for mode in (0, 1, 2):
+        renderer.trace_rays_static(_rays(30000, 12 + mode, mode), mode, 3)
+    assert count() == before
+    renderer.trace_rays(rays, 0, 3)
+    assert count() > before
