@@ -101,6 +101,8 @@ struct Rng {
         x = mod_m(uint64_t(x) * 48271ull);
         return x;
     }
+    // Three steps at once: x * 48271^3 mod (2^31 - 1), 48271^3 mod (2^31 - 1) = 1291394886.
+    LUX_HDI void skip3() { x = mod_m(uint64_t(x) * 1291394886ull); }
     // (float(x - 1) / (1 + float(max - min))) * (1 - 0) + 0; the divisor rounds to 2^31
     LUX_DI float u01() {
         uint32_t v = next();

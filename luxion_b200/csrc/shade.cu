@@ -314,8 +314,19 @@ LUX_DI void lobe_probs(f3 wo, f3 n, float metal, f3 color, float ior, float tran
     pD = (1.0f - pR) * (1.0f - sr) * (1.0f - metal);
     pS = 1.0f - pR - pD;
 }
-// sampleCookTorrance (src/shaders/cook_torrance.cu:156-224)
-LUX_DI f3 sample_ct(f3 wo, f3 n, float rough, float metal, Rng& rng, f3 color, float ior, float trans) {
+// The lobe probabilities depend on the outgoing direction and the material only, so one
+// evaluation serves the direction sampling and every pdf of a shading point (the reference
+// evaluates them in each call, with the same operands).
+struct Lobes {
+    float pR, pD, pS;
+};
+LUX_DI Lobes lobes_of(f3 wo, f3 n, float metal, f3 color, float ior, float trans) {
+    Lobes L;
+    lobe_probs(wo, n, metal, color, gmax(ior, 1.0001f), trans, L.pR, L.pD, L.pS);
+    return L;
+}
+// sampleCookTorrance (src/shaders/cook_torrance.cu:156-224); L = lobes_of(wo, n, metal, color, ior, trans)
+LUX_DI f3 sample_ct(f3 wo, f3 n, float rough, Rng& rng, float ior, const Lobes& L) {
     float r = rng.u01();
     ior = gmax(ior, 1.0001f);
     rough = gclamp(rough, 0.0001f, 1.0f);
@@ -323,8 +334,7 @@ LUX_DI f3 sample_ct(f3 wo, f3 n, float rough, float metal, Rng& rng, f3 color, f
     bool enter = dot(wo, n) > 0.0f;
     f3 nf = enter ? n : -n;
     float etaI = enter ? 1.0f : ior, etaT = enter ? ior : 1.0f;
-    float pR, pD, pS;
-    lobe_probs(wo, n, metal, color, ior, trans, pR, pD, pS);
+    const float pD = L.pD, pS = L.pS;
     if (r > pS && r <= pS + pD) return hemisphere(nf, rng);
     float x1 = rng.u01(), x2 = rng.u01();
     float th = atanf((alpha * sqrtf(x1)) / sqrtf(1.0f - x1));
@@ -360,16 +370,15 @@ LUX_DI float pdf_ggx_t(f3 wo, f3 wi, f3 n, float rough, float ior) {
     float ph = D_GGX(ht, n, alpha) * fabsf(dot(n, ht));
     return ph * (etaT * etaT * fabsf(dot(wi, ht))) / gmax(den * den, kEPS_CT);
 }
-LUX_DI float PDF(f3 wo, f3 wi, f3 n, float rough, float metal, f3 color, float ior, float trans) {
+// L = lobes_of(wo, n, metal, color, ior, trans)
+LUX_DI float PDF(f3 wo, f3 wi, f3 n, float rough, float ior, const Lobes& L) {
     ior = gmax(ior, 1.0001f);
     f3 nf = dot(wo, n) < 0.0f ? -n : n;
     float pdfD = fmaxf(0.0f, dot(wi, nf)) * kINV_PI;
     float pdfS = pdf_ggx(wo, wi, nf, rough);
     float pdfR = pdf_ggx_t(wo, wi, n, rough, ior);
     bool refr = (dot(wi, n) * dot(wo, n)) < 0.0f;
-    float pR, pD, pS;
-    lobe_probs(wo, n, metal, color, ior, trans, pR, pD, pS);
-    float pdf = refr ? pR * pdfR : pD * pdfD + pS * pdfS;
+    float pdf = refr ? L.pR * pdfR : L.pD * pdfD + L.pS * pdfS;
     return gmax(pdf, kPDF_CLAMP);
 }
 LUX_DI f3 shade_ct(f3 wo, f3 albedo, f3 n, f3 wi, float rough, float metal, float ior, float trans) {
@@ -403,12 +412,29 @@ LUX_DI f3 env_lookup(const DevScene& S, f3 d, float intensity) {
     return mk(e.x, e.y, e.z) * intensity;
 }
 
-// sampleDirectLight for one path (src/kernels/sample_direct_light.cu:31-100)
-LUX_DI f3 light_sample(const DevScene& S, const DevOptions& O, int iter, int pixel, int depth, f3& env_dir) {
+// NEE mode of a kernel instantiation: -1 = read from the options at run time, 0 = none,
+// 1 = emitter sampling only (-dmis), 2 = environment sampling (-emis, with or without -dmis;
+// the reference's shading then takes the environment branch, src/kernels/shade_path.cu:166-249).
+template <int NEE> LUX_DI bool nee_env(const DevOptions& O) { return NEE < 0 ? O.env != 0 : NEE == 2; }
+template <int NEE> LUX_DI bool nee_dl(const DevOptions& O) {
+    return NEE < 0 ? O.dl != 0 : (NEE == 1 || (NEE == 2 && O.dl != 0));
+}
+inline int nee_mode_of(const DevOptions& O) { return O.env ? 2 : (O.dl ? 1 : 0); }
+
+// sampleDirectLight for one path (src/kernels/sample_direct_light.cu:31-100). With both -dmis
+// and -emis the reference draws the emitter point and then keeps only the environment
+// direction (the shading reads one of the two); want_dl = false skips the emitter point's CDF
+// searches and vertex loads and only advances the random stream past its three draws.
+template <int NEE = -1>
+LUX_DI f3 light_sample(const DevScene& S, const DevOptions& O, int iter, int pixel, int depth, f3& env_dir,
+                       bool want_dl = true) {
     Rng rng = Rng::seeded(iter, pixel, depth);
     f3 dl = mk(0.0f, 0.0f, 0.0f);
     env_dir = mk(0.0f, 0.0f, 0.0f);
-    if (O.dl) {
+    const bool dl_on = nee_dl<NEE>(O);
+    if (dl_on && !want_dl) {
+        rng.skip3();
+    } else if (dl_on) {
         float rnd = rng.u01();
         int sel = select_from_cdf(S.emissive_prefix, S.num_emissive, rnd);
         int ii = __ldg(S.emissive_inst + sel);
@@ -428,7 +454,7 @@ LUX_DI f3 light_sample(const DevScene& S, const DevOptions& O, int iter, int pix
         f3 lp = u * v0 + v * v1 + (1.0f - u - v) * v2;
         dl = xform(I.M, lp, 1.0f);
     }
-    if (O.env) {
+    if (nee_env<NEE>(O)) {
         float rnd = rng.u01();
         const int H = S.env_h, W = S.env_w;
         int mg = select_from_cdf_guided(S.marginal, S.marginal_guide, S.guide_marg, rnd);
@@ -449,20 +475,41 @@ LUX_DI f3 light_sample(const DevScene& S, const DevOptions& O, int iter, int pix
     return dl;
 }
 
+// A path as shade_one sees it. d, thr, spec, pixel and iter are read on entry; the other
+// fields are outputs: the new origin, radiance and pdf of a surviving path (color always).
 struct PathState {
-    f3 o, d, thr, color, nee;
+    f3 o, d, thr, color;
     float last_pdf;
     bool spec;
     int pixel, iter;
 };
 
+// The path fields shade_one reads late, loaded where they are used instead of being held in
+// registers across the shading (origin, radiance so far, pdf of the last bounce, NEE sample).
+struct WavePathIn {
+    const DevWave& W;
+    int pid;
+    LUX_DI f3 origin() const { float4 a = W.s0[pid]; return mk(a.x, a.y, a.z); }
+    LUX_DI float last_pdf() const { return W.s0[pid].w; }
+    LUX_DI f3 color0() const { float4 a = W.s3[pid]; return mk(a.x, a.y, a.z); }
+    LUX_DI f3 nee() const { float4 a = W.s4[pid]; return mk(a.x, a.y, a.z); }
+};
+
 // shadePath for one path; returns true if the path survives (is not killed).
 // sh_t: DL shadow hit t (or env occlusion); sh_* the DL shadow hit record.
 // MATDBG: the instantiation that also renders the material debug views (O.material_debug).
-template <bool MATDBG>
-LUX_DI bool shade_one(const DevScene& S, const DevOptions& O, int depth, PathState& p, float t, int inst, int prim,
-                      float bu, float bv, float sh_t, int sh_inst, int sh_prim, float sh_u, float sh_v) {
+// NEE: as for light_sample. At most one radiance term is added per call (emission, the NEE
+// contribution or the environment on a miss), so p.color = color0 + that term.
+// SPAWN_KILLED: also sample the next direction and spawn the ray of a path that an emitter
+// hit kills, as the reference does (its result is then unused; the parity entry reports it).
+// The NEE terms draw no random numbers, so sampling the direction after them leaves the
+// random stream as the reference's (sample first, then Russian roulette).
+template <bool MATDBG, int NEE, bool SPAWN_KILLED, class In>
+LUX_DI bool shade_one(const DevScene& S, const DevOptions& O, int depth, PathState& p, const In& in, float t, int inst,
+                      int prim, float bu, float bv, float sh_t, int sh_inst, int sh_prim, float sh_u, float sh_v) {
     Rng rng = Rng::seeded(p.iter, p.pixel, depth);
+    f3 add = mk(0.0f, 0.0f, 0.0f);
+    bool added = false;
     const bool has_exr = S.has_env != 0;
     bool kill = false;
     if (inst >= 0 && t > 0.0f) {
@@ -482,36 +529,38 @@ LUX_DI bool shade_one(const DevScene& S, const DevOptions& O, int depth, PathSta
         bool is_spec = rough < kSPEC_ROUGH;
         f3 nf = dot(-p.d, normal) < 0.0f ? -normal : normal;
         const float ior = m.ior, trans = m.transmission;
-        f3 sd = sample_ct(-p.d, normal, rough, metal, rng, mc, ior, trans);
         bool emissive = length(emission) > kEPS_UTIL;
-        if (O.env) {
+        const Lobes L = lobes_of(-p.d, normal, metal, mc, ior, trans);
+        if (nee_env<NEE>(O)) {
             if (emissive) {
                 float w = 1.0f;
                 if (depth > 1 && !p.spec) {
-                    float pb = p.last_pdf;
+                    float pb = in.last_pdf();
                     float pe = envmap_pdf(S, p.d);
                     w = (pb * pb) / (pb * pb + pe * pe);
                 }
-                p.color = p.color + p.thr * (w * emission);
+                add = p.thr * (w * emission);
+                added = true;
                 kill = true;
             } else if (sh_t < 0.0f && !is_spec && has_exr) {
-                f3 ed = p.nee;
+                f3 ed = in.nee();
                 float pee = envmap_pdf(S, ed);
-                float pbe = PDF(-p.d, ed, normal, rough, metal, mc, ior, trans);
+                float pbe = PDF(-p.d, ed, normal, rough, ior, L);
                 float w = (pee * pee) / (pee * pee + pbe * pbe);
                 f3 brdf = BRDF(-p.d, normal, ed, mc, rough, metal, ior, trans);
                 f3 el = env_lookup(S, normalize(ed), O.env_intensity);
                 float cs = dot(nf, ed);
                 if (cs > 0.0f && pee > 1e-8f) {
                     f3 contrib = (el * brdf * cs) / pee;
-                    p.color = p.color + p.thr * contrib * w;
+                    add = p.thr * contrib * w;
+                    added = true;
                 }
             }
-        } else if (O.dl) {
+        } else if (nee_dl<NEE>(O)) {
             if (emissive) {
                 float w = 1.0f;
                 if (depth > 1 && !p.spec) {
-                    float pb = p.last_pdf;
+                    float pb = in.last_pdf();
                     float dsq = is.t * is.t;
                     float cl = dot(is.normal, -p.d);
                     if (cl > 0.0001f) {
@@ -522,12 +571,13 @@ LUX_DI bool shade_one(const DevScene& S, const DevOptions& O, int depth, PathSta
                         w = 0.0f;
                     }
                 }
-                p.color = p.color + p.thr * (w * emission);
+                add = p.thr * (w * emission);
+                added = true;
                 kill = true;
             } else if (sh_inst >= 0 && sh_t > 0.0f && !is_spec) {
                 Isect dli = ch_direct_light(S, sh_t, sh_inst, sh_prim, sh_u, sh_v);
-                f3 sp = is.t * p.d + p.o;
-                f3 lv = p.nee - sp;
+                f3 sp = is.t * p.d + in.origin();
+                f3 lv = in.nee() - sp;
                 float dsq = dot(lv, lv);
                 float dist = sqrtf(dsq);
                 f3 ld = lv / dist;
@@ -536,24 +586,31 @@ LUX_DI bool shade_one(const DevScene& S, const DevOptions& O, int depth, PathSta
                 if (cs > 0.0f && cl > 0.0f) {
                     float pa = 1.0f / S.total_area;
                     float ps = pa * (dsq / cl);
-                    float pb = PDF(-p.d, ld, normal, rough, metal, mc, ior, trans);
+                    float pb = PDF(-p.d, ld, normal, rough, ior, L);
                     float w = (ps * ps) / (ps * ps + pb * pb);
                     f3 brdf = BRDF(-p.d, normal, ld, mc, rough, metal, ior, trans);
                     const DevMaterial& lm = S.mats[dli.material];
                     f3 lr = get_emission(lm, dli.u, dli.v);
                     f3 contrib = (lr * brdf * cs) / ps;
-                    p.color = p.color + p.thr * contrib * w;
+                    add = p.thr * contrib * w;
+                    added = true;
                 }
             }
         } else if (emissive) {
-            p.color = p.color + p.thr * emission;
+            add = p.thr * emission;
+            added = true;
             kill = true;
         }
+        if (kill && !SPAWN_KILLED) {
+            p.color = in.color0() + add;
+            return false;
+        }
+        f3 sd = sample_ct(-p.d, normal, rough, rng, ior, L);
         if (!kill) {
             bool transmitted = dot(-p.d, normal) * dot(sd, normal) < 0.0f;
             bool spec = is_spec || transmitted;
             f3 f = shade_ct(-p.d, mc, normal, sd, rough, metal, ior, trans);
-            float pdf = PDF(-p.d, sd, normal, rough, metal, mc, ior, trans);
+            float pdf = PDF(-p.d, sd, normal, rough, ior, L);
             p.thr = p.thr * (f / pdf);
             p.last_pdf = pdf;
             p.spec = spec;
@@ -564,8 +621,9 @@ LUX_DI bool shade_one(const DevScene& S, const DevOptions& O, int depth, PathSta
                 else p.thr = p.thr / surv;
             }
         }
+        p.color = added ? in.color0() + add : in.color0();
         // ray spawn (shade_path.cu:333-353), run for paths killed above as well
-        f3 hp = p.o + (is.t - .0001f) * normalize(p.d);
+        f3 hp = in.origin() + (is.t - .0001f) * normalize(p.d);
         float sl2 = dot(sd, sd);
         if (!(sl2 > 1e-12f) || !isfinite(sl2)) return false;
         p.d = sd;
@@ -577,28 +635,27 @@ LUX_DI bool shade_one(const DevScene& S, const DevOptions& O, int depth, PathSta
         f3 d = normalize(p.d);
         f3 er = env_lookup(S, d, O.env_intensity);
         float w = 1.0f;
-        if (O.env && depth > 1 && !p.spec) {
-            float pb = p.last_pdf;
+        if (nee_env<NEE>(O) && depth > 1 && !p.spec) {
+            float pb = in.last_pdf();
             float pe = envmap_pdf(S, d);
             w = (pb * pb) / (pb * pb + pe * pe);
         }
-        p.color = p.color + p.thr * er * w;
+        add = p.thr * er * w;
+        added = true;
     }
+    p.color = added ? in.color0() + add : in.color0();
     return false;
 }
 
+// The fields shade_one reads on entry.
 LUX_DI PathState load_path(const DevWave& W, int pid) {
-    float4 a = W.s0[pid], b = W.s1[pid], c = W.s2[pid], d = W.s3[pid], e = W.s4[pid];
+    float4 b = W.s1[pid], c = W.s2[pid];
     PathState p;
-    p.o = mk(a.x, a.y, a.z);
-    p.last_pdf = a.w;
     p.d = mk(b.x, b.y, b.z);
     p.spec = (__float_as_int(b.w) & 1) != 0;
     p.thr = mk(c.x, c.y, c.z);
     p.pixel = __float_as_int(c.w);
-    p.color = mk(d.x, d.y, d.z);
-    p.iter = __float_as_int(d.w);
-    p.nee = mk(e.x, e.y, e.z);
+    p.iter = __float_as_int(W.s3[pid].w);
     return p;
 }
 
@@ -622,7 +679,7 @@ __global__ void __launch_bounds__(kShadeBlock, 16) k_camera(DevScene S, DevWave 
         W.s3[pid] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(iter));
         if (nee) {
             f3 ed;
-            f3 dl = light_sample(S, O, iter, index, 0, ed);
+            f3 dl = light_sample(S, O, iter, index, 0, ed, !O.env);
             f3 v = O.env ? ed : dl;
             W.s4[pid] = make_float4(v.x, v.y, v.z, 0.0f);
         }
@@ -637,14 +694,14 @@ __global__ void __launch_bounds__(kShadeBlock, 16) k_camera(DevScene S, DevWave 
 // texture fetches and gathers, and hiding that latency with more warps pays more than the
 // register spills cost (shade per 16-spp step of the 1M-triangle 1080p workload: 28.3 ms at
 // 5 blocks per SM, 22.6 at 8, 20.4 at 12, 18.8 at 16).
-template <bool JOBS, bool MATDBG>
+template <bool JOBS, bool MATDBG, int NEE>
 __global__ void __launch_bounds__(kShadeBlock, 16) k_shade(const __grid_constant__ DevScene S0, DevWave W, DevOptions O,
                                                        int bounce, int compact) {
     const int n = *(volatile int*)&W.ctr->count[bounce];
     const int depth = bounce + 1;
     const int* q = W.queue[bounce & 1];
     int* nq = W.queue[(bounce + 1) & 1];
-    const bool nee = O.dl || O.env;
+    const bool nee = nee_dl<NEE>(O) || nee_env<NEE>(O);
     const int lane = threadIdx.x & 31;
     const int stride = gridDim.x * blockDim.x;
     // uniform trip count across the warp so the append below runs converged
@@ -671,14 +728,16 @@ __global__ void __launch_bounds__(kShadeBlock, 16) k_shade(const __grid_constant
             if (nee && inst >= 0) {
                 float4 sh = W.sh_hit[slot];
                 sh_t = sh.x;
-                if (O.dl && !O.env) {
+                if (!nee_env<NEE>(O)) {
                     su = sh.y;
                     sv = sh.z;
                     si = __float_as_int(sh.w);
                     spr = W.sh_prim[slot];
                 }
             }
-            alive = shade_one<MATDBG>(S, O, depth, p, h.x, inst, prim, h.y, h.z, sh_t, si, spr, su, sv) && job_compact;
+            alive = shade_one<MATDBG, NEE, false>(S, O, depth, p, WavePathIn{W, pid}, h.x, inst, prim, h.y, h.z, sh_t, si, spr,
+                                           su, sv) &&
+                    job_compact;
             W.s3[pid] = make_float4(p.color.x, p.color.y, p.color.z, __int_as_float(p.iter));
             if (alive) {
                 W.s0[pid] = make_float4(p.o.x, p.o.y, p.o.z, p.last_pdf);
@@ -686,8 +745,8 @@ __global__ void __launch_bounds__(kShadeBlock, 16) k_shade(const __grid_constant
                 W.s2[pid] = make_float4(p.thr.x, p.thr.y, p.thr.z, __int_as_float(p.pixel));
                 if (nee) {
                     f3 ed;
-                    f3 dl = light_sample(S, O, p.iter, p.pixel, depth, ed);
-                    f3 v = O.env ? ed : dl;
+                    f3 dl = light_sample<NEE>(S, O, p.iter, p.pixel, depth, ed, !nee_env<NEE>(O));
+                    f3 v = nee_env<NEE>(O) ? ed : dl;
                     W.s4[pid] = make_float4(v.x, v.y, v.z, 0.0f);
                 }
             }
@@ -783,7 +842,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_camera_jobs(DevWave W, DevOptio
         W.s3[pid] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(iter));
         if (nee) {
             f3 ed;
-            f3 dl = light_sample(W.scenes[J.scene], O, iter, index, 0, ed);
+            f3 dl = light_sample(W.scenes[J.scene], O, iter, index, 0, ed, !O.env);
             f3 v = O.env ? ed : dl;
             W.s4[pid] = make_float4(v.x, v.y, v.z, 0.0f);
         }
@@ -877,6 +936,17 @@ __global__ void k_tonemap(const float* __restrict__ image, uchar4* __restrict__ 
 }
 
 // ---- kernel-level parity entry points ------------------------------------------------
+// Path rows of 24 floats: origin 0-2, direction 3-5, radiance 6-8, throughput 9-11, DL point
+// 12-14, env direction 15-17, pixel 18, killed 19, specular 20, pdf 21.
+struct RowPathIn {
+    const float* f;
+    bool env;
+    LUX_DI f3 origin() const { return mk(f[0], f[1], f[2]); }
+    LUX_DI float last_pdf() const { return f[21]; }
+    LUX_DI f3 color0() const { return mk(f[6], f[7], f[8]); }
+    LUX_DI f3 nee() const { return env ? mk(f[15], f[16], f[17]) : mk(f[12], f[13], f[14]); }
+};
+
 __global__ void k_shade_ext(DevScene S, DevOptions O, float* paths, const uint32_t* hits, int n, int iter, int depth,
                             int compact, int* survivors, int* n_out) {
     const int lane = threadIdx.x & 31;
@@ -888,9 +958,7 @@ __global__ void k_shade_ext(DevScene S, DevOptions O, float* paths, const uint32
             PathState p;
             p.o = mk(f[0], f[1], f[2]);
             p.d = mk(f[3], f[4], f[5]);
-            p.color = mk(f[6], f[7], f[8]);
             p.thr = mk(f[9], f[10], f[11]);
-            p.nee = O.env ? mk(f[15], f[16], f[17]) : mk(f[12], f[13], f[14]);
             p.pixel = __float_as_int(f[18]);
             p.spec = f[20] != 0.0f;
             p.last_pdf = f[21];
@@ -901,8 +969,9 @@ __global__ void k_shade_ext(DevScene S, DevOptions O, float* paths, const uint32
             float su = __uint_as_float(h[8]), sv = __uint_as_float(h[9]);
             int si = int(h[6]), spr = int(h[7]);
             if (O.env) si = -1;
-            bool survived = shade_one<true>(S, O, depth, p, t, inst, prim, __uint_as_float(h[3]), __uint_as_float(h[4]),
-                                      __uint_as_float(h[5]), si, spr, su, sv);
+            bool survived = shade_one<true, -1, true>(S, O, depth, p, RowPathIn{f, O.env != 0}, t, inst, prim,
+                                                __uint_as_float(h[3]), __uint_as_float(h[4]), __uint_as_float(h[5]), si,
+                                                spr, su, sv);
             alive = survived && compact;
             f[0] = p.o.x; f[1] = p.o.y; f[2] = p.o.z;
             f[3] = p.d.x; f[4] = p.d.y; f[5] = p.d.z;
@@ -961,8 +1030,8 @@ int shade_grid_blocks() {
         int sms = 0, per = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         int per_jobs = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_shade<false, false>, kShadeBlock, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_jobs, k_shade<true, false>, kShadeBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_shade<false, false, 2>, kShadeBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_jobs, k_shade<true, false, 2>, kShadeBlock, 0);
         per = std::min(per, per_jobs);
         cached = sms * (per > 0 ? per : 1);
     }
@@ -979,9 +1048,18 @@ cudaError_t launch_camera(const DevScene& S, const DevWave& W, const DevOptions&
 
 cudaError_t launch_shade(const DevScene& S, const DevWave& W, const DevOptions& O, int bounce, int compact,
                          cudaStream_t st) {
-    if (W.path_job) k_shade<true, false><<<shade_grid_blocks(), kShadeBlock, 0, st>>>(S, W, O, bounce, compact);
-    else if (O.material_debug) k_shade<false, true><<<shade_grid_blocks(), kShadeBlock, 0, st>>>(S, W, O, bounce, compact);
-    else k_shade<false, false><<<shade_grid_blocks(), kShadeBlock, 0, st>>>(S, W, O, bounce, compact);
+    const int g = shade_grid_blocks(), mode = nee_mode_of(O);
+    if (O.material_debug && !W.path_job) {
+        k_shade<false, true, -1><<<g, kShadeBlock, 0, st>>>(S, W, O, bounce, compact);
+    } else if (W.path_job) {
+        if (mode == 2) k_shade<true, false, 2><<<g, kShadeBlock, 0, st>>>(S, W, O, bounce, compact);
+        else if (mode == 1) k_shade<true, false, 1><<<g, kShadeBlock, 0, st>>>(S, W, O, bounce, compact);
+        else k_shade<true, false, 0><<<g, kShadeBlock, 0, st>>>(S, W, O, bounce, compact);
+    } else {
+        if (mode == 2) k_shade<false, false, 2><<<g, kShadeBlock, 0, st>>>(S, W, O, bounce, compact);
+        else if (mode == 1) k_shade<false, false, 1><<<g, kShadeBlock, 0, st>>>(S, W, O, bounce, compact);
+        else k_shade<false, false, 0><<<g, kShadeBlock, 0, st>>>(S, W, O, bounce, compact);
+    }
     return cudaGetLastError();
 }
 
