@@ -303,7 +303,9 @@ int lux_wave_counts(lux_ctx* ctx, int* paths, int* shadow, int max_bounces);
 /* Closest-hit / any-hit trace of caller rays through the device BVH.
  * rays: n * 8 floats (origin xyz, tmax, direction xyz, pixel-as-float-bits).
  * mode 0: closest hit (radiance; pixel and iter key the alpha-blend hash);
- * mode 1: closest hit with tmax (DL shadow); mode 2: any hit (env shadow).
+ * mode 1: closest hit with tmax (DL shadow); mode 2: any hit (env shadow);
+ * mode 3: closest hit as mode 0, counting the traversal's work (the BVH heatmap's count, node
+ * visits plus triangle tests), which replaces u: word 3 holds the count, word 4 is 0.
  * hits: n * 5 words (t as f32 bits, instance, prim, u bits, v bits); t=-1 on a miss; for
  * mode 2 only word 0 is meaningful (1.0 occluded, -1.0 free). Host buffers. */
 int lux_trace_rays(lux_ctx* ctx, const float* rays, int n, int mode, int iter, uint32_t* hits);

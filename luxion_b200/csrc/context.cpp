@@ -1242,7 +1242,7 @@ int lux_wave_counts(lux_ctx* C, int* paths, int* shadow, int max_bounces) {
 
 // ---- kernel-level entry points -------------------------------------------------------
 int lux_trace_rays(lux_ctx* C, const float* rays, int n, int mode, int iter, uint32_t* hits) {
-    if (!C || (!rays && n > 0) || (!hits && n > 0) || n < 0 || mode < 0 || mode > 2)
+    if (!C || (!rays && n > 0) || (!hits && n > 0) || n < 0 || mode < 0 || mode > 3)
         return fail(LUX_ERR_INVALID, "bad arguments");
     if (n == 0) return LUX_OK;
     cudaSetDevice(C->device);
@@ -1264,7 +1264,7 @@ int lux_trace_rays(lux_ctx* C, const float* rays, int n, int mode, int iter, uin
 }
 
 int lux_trace_rays_static(lux_ctx* C, const float* rays, int n, int mode, int iter, uint32_t* hits) {
-    if (!C || (!rays && n > 0) || (!hits && n > 0) || n < 0 || mode < 0 || mode > 2)
+    if (!C || (!rays && n > 0) || (!hits && n > 0) || n < 0 || mode < 0 || mode > 3)
         return fail(LUX_ERR_INVALID, "bad arguments");
     if (n > LUX_TRACE_STATIC_MAX_RAYS)
         return fail(LUX_ERR_INVALID, "lux_trace_rays_static: n = " + std::to_string(n) +

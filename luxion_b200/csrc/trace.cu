@@ -62,11 +62,19 @@ struct TRay {
 
 // Reciprocal for the box tests only (the triangle test uses the direction itself): the
 // hardware approximation, at most 1 ulp off, scales both slab distances of an axis by the same
-// factor within 2^-23 of 1, far inside the 2^-17 acceptance margin. A subnormal component
-// flushes to a signed zero, giving a signed infinity like an exact zero.
+// factor within 2^-23 of 1, far inside the 2^-17 acceptance margin.
+// A component below 2^-66 in magnitude (zero and subnormals included) is raised to 2^-66 with
+// its sign. An exact zero would give an infinite reciprocal, that axis's slab distances would
+// then be NaN, and fminf / fmaxf drop NaN operands: the axis would stop culling, and in a
+// world-space tree the ray would sweep a whole slab of the scene (a camera on an axis-aligned
+// plane makes such rays, one pixel column of them). With 2^-66 the axis culls every box that
+// does not hold the origin's coordinate to within 2^-66 * tmax, and keeps every box that holds
+// it with a margin m for t up to m * 2^66: boxes are padded by far more than the 2^-66 * t a
+// ray this close to the axis plane drifts within the scene.
 LUX_DI float rcp_box(float x) {
+    const float c = copysignf(fmaxf(fabsf(x), 1.35525271560688054e-20f), x);  // 2^-66
     float r;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(c));
     return r;
 }
 
@@ -556,6 +564,12 @@ __global__ void __launch_bounds__(kTraceBlock, 7) k_trace(const __grid_constant_
                         h[0] = __float_as_uint(L.best.inst >= 0 ? 1.0f : -1.0f);
                         h[1] = h[2] = 0xffffffffu;
                         h[3] = h[4] = 0u;
+                    } else if (MODE == 3) {
+                        h[0] = __float_as_uint(L.best.inst >= 0 ? L.best.t : -1.0f);
+                        h[1] = uint32_t(L.best.inst);
+                        h[2] = uint32_t(L.best.prim);
+                        h[3] = uint32_t(L.work);
+                        h[4] = 0u;
                     } else {
                         h[0] = __float_as_uint(L.best.inst >= 0 ? L.best.t : -1.0f);
                         h[1] = uint32_t(L.best.inst);

@@ -172,3 +172,49 @@ def test_furnace_energy(kind, emis):
     assert frac >= PIXEL_FRAC and relmse <= RELMSE_TOL, (frac, relmse)
     want = expected_furnace_image(o, s, kind, 64)
     assert abs(float(img.mean()) - float(want.mean())) < 1e-3, (img.mean(), want.mean())
+
+
+def test_c2_zero_direction_components(c2):
+    """Rays with direction components of exactly zero. The C2 camera at (0, 7, 25) looks at
+    (0, 1, 0), so view, up and right have exact zeros, and a camera ray whose jittered pixel
+    offset rounds to 0 has d.x = 0 (about 3e-5 of the samples of one pixel column). Such a
+    component once made the box tests' reciprocal infinite and that axis stop culling, so in the
+    single-level layout the ray swept a slab of the whole scene. Hits stay bit-exact (also with
+    subnormal components), and the traversal work (lux_trace_rays mode 3: node visits plus
+    triangle tests) is that of the same rays with the component at 1e-6 instead."""
+    s, r, o, opt, pix = c2
+    cam = s.desc.camera
+    rng = np.random.default_rng(7)
+    n = 2048
+    rays = np.zeros((n, 8), np.float32)
+    rays[:, 0:3] = np.array(cam.position[:], np.float32)
+    rays[n // 2:, 0:3] += rng.uniform(-8, 8, (n - n // 2, 3)).astype(np.float32)
+    view, up = np.array(cam.view[:], np.float64), np.array(cam.up[:], np.float64)
+    py = rng.uniform(-0.5, 0.5, n) * float(cam.height) * float(cam.pixel_length[1])
+    d = view[None, :] - up[None, :] * py[:, None]
+    d[:, 0] = 0.0
+    # a quarter of them along the y or z axis (two zero components)
+    k = n // 4
+    d[:k] = np.eye(3)[rng.integers(1, 3, k)] * rng.choice([-1.0, 1.0], (k, 1))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rays[:, 4:7] = d.astype(np.float32)
+    rays[:, 3] = 1e16
+    rays[:, 7] = np.arange(n, dtype=np.int32).view(np.float32)
+    assert np.all(rays[:, 4] == 0.0)
+    subnormal = rays.copy()
+    subnormal[:, 4] = np.float32(1e-40) * rng.choice([-1.0, 1.0], n).astype(np.float32)
+    for case in (rays, subnormal):
+        for mode in (0, 2):
+            hg, ho = r.trace_rays(case, mode, 2), o.trace(case, mode, 2)
+            if mode == 2:
+                hg, ho = hg[:, :1], ho[:, :1]
+            assert np.array_equal(hg, ho), mode
+    w0 = r.trace_rays(rays, 3, 2)
+    assert np.array_equal(w0[:, :3], r.trace_rays(rays, 0, 2)[:, :3])
+    nudged = rays.copy()
+    nudged[:, 4] = np.float32(1e-6)
+    w1 = r.trace_rays(nudged, 3, 2)
+    work, work_nudged = w0[:, 3].astype(np.float64), w1[:, 3].astype(np.float64)
+    assert work.mean() > 5
+    assert work.sum() <= 1.25 * work_nudged.sum() + 10 * n, (work.sum(), work_nudged.sum())
+    assert work.max() <= 4 * work_nudged.max() + 200, (work.max(), work_nudged.max())
