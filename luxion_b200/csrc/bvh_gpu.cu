@@ -1308,13 +1308,16 @@ int build_bvh8_device(const float* d_boxes, const std::vector<int>& tree_begin, 
     if (!d_tb || !ord[0] || !ord[1] || !ord_fin || !bn || !large[0] || !large[1] || !small || !ctr || !slots ||
         !bin_cnt || !bin_lo || !bin_hi || !chunk_slot || !chunk_start || !chunk_left || !chunk_lbase)
         return fail(LUX_ERR_OOM, "BVH build: device scratch allocation failed");
-    LUX_CUDA(cudaMallocHost(&h_ctr, 8 * sizeof(int)));
-    struct HostFree {
+    h_ctr = static_cast<int*>(pinned_get(8 * sizeof(int)));
+    if (!h_ctr) return fail(LUX_ERR_OOM, "BVH build: page-locked host allocation failed");
+    struct HostFree {  // back to the pool once no copy into it can still be queued
         int* p;
+        cudaStream_t st;
         ~HostFree() {
-            if (p) cudaFreeHost(p);
+            cudaStreamSynchronize(st);
+            pinned_put(p, 8 * sizeof(int));
         }
-    } hf{h_ctr};
+    } hf{h_ctr, st};
     LUX_CUDA(cudaMemcpyAsync(d_tb, tree_begin.data(), sizeof(int) * (G + 1), cudaMemcpyHostToDevice, st));
     LUX_CUDA(cudaMemsetAsync(ctr, 0, 8 * sizeof(int), st));
     // every index array starts in range, so no read can leave its buffer whatever is computed

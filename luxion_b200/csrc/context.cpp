@@ -32,8 +32,10 @@
 #include <cstring>
 #include <functional>
 #include <map>
+#include <mutex>
 #include <string>
 #include <thread>
+#include <tuple>
 #include <vector>
 
 using namespace lux;
@@ -238,8 +240,7 @@ int make_texture(const lux_texture_desc& t, DevTex& out, int storage, TexStage& 
         default:
             return fail(LUX_ERR_INVALID, "unknown texture format");
     }
-    LUX_CUDA(cudaMallocArray(&out.arr, &fd, t.width, t.height));
-    note_device_alloc();
+    LUX_CUDA(tex_array_get(&out.arr, fd, size_t(t.width), size_t(t.height)));
     if (dev_src)
         LUX_CUDA(cudaMemcpy2DToArrayAsync(out.arr, 0, 0, dev_src, size_t(t.width) * texel, size_t(t.width) * texel,
                                           t.height, cudaMemcpyDeviceToDevice, stage.st));
@@ -610,6 +611,8 @@ int build_scene(lux_scene* R, const lux_scene_desc& d, const lux_options& opt, c
 void scene_release(lux_scene* R) {
     if (!R || --R->refs > 0) return;
     cudaSetDevice(R->device);
+    // no copy into the textures is left in flight when their arrays go back for reuse
+    if (R->stream) cudaStreamSynchronize(R->stream);
     for (auto& t : R->texs) destroy_texture(t);
     destroy_texture(R->env);
     for (void* p : R->allocs) scratch_free(p, R->stream);
@@ -757,13 +760,15 @@ int run_waves(lux_ctx* C, int first_iter, int n_iter) {
     const int spw = C->spp_per_wave;
     const int nwaves = (n_iter + spw - 1) / spw;
     if (C->h_cap < nwaves) {
-        if (C->h_ctr) cudaFreeHost(C->h_ctr);
-        if (C->h_wave_iter) cudaFreeHost(C->h_wave_iter);
+        // the previous call ended with a synchronize, so no copy uses the old blocks
+        pinned_put(C->h_ctr, sizeof(WaveCounters) * size_t(C->h_cap));
+        pinned_put(C->h_wave_iter, sizeof(int) * 2 * size_t(C->h_cap));
         C->h_ctr = nullptr;
         C->h_wave_iter = nullptr;
         C->h_cap = 0;
-        LUX_CUDA(cudaMallocHost(&C->h_ctr, sizeof(WaveCounters) * nwaves));
-        LUX_CUDA(cudaMallocHost(&C->h_wave_iter, sizeof(int) * 2 * nwaves));
+        C->h_ctr = static_cast<WaveCounters*>(pinned_get(sizeof(WaveCounters) * size_t(nwaves)));
+        C->h_wave_iter = static_cast<int*>(pinned_get(sizeof(int) * 2 * size_t(nwaves)));
+        if (!C->h_ctr || !C->h_wave_iter) return fail(LUX_ERR_OOM, "page-locked host allocation failed");
         C->h_cap = nwaves;
     }
     const int epw = events_needed(C);
@@ -897,6 +902,100 @@ std::atomic<int64_t> g_device_allocs{0};
 }
 
 void lux::note_device_alloc() { g_device_allocs.fetch_add(1, std::memory_order_relaxed); }
+
+namespace {
+std::mutex g_pinned_mu;
+std::map<size_t, std::vector<void*>> g_pinned_free;
+size_t pinned_class(size_t bytes) {
+    size_t c = 256;
+    while (c < bytes) c <<= 1;
+    return c;
+}
+}  // namespace
+
+void* lux::pinned_get(size_t bytes) {
+    const size_t c = pinned_class(bytes);
+    {
+        std::lock_guard<std::mutex> lk(g_pinned_mu);
+        auto it = g_pinned_free.find(c);
+        if (it != g_pinned_free.end() && !it->second.empty()) {
+            void* p = it->second.back();
+            it->second.pop_back();
+            return p;
+        }
+    }
+    void* p = nullptr;
+    if (cudaMallocHost(&p, c) != cudaSuccess) return nullptr;
+    return p;
+}
+
+namespace {
+struct TexShape {
+    int device, x, y, z, w, kind;
+    size_t width, height;
+    bool operator<(const TexShape& o) const {
+        return std::tie(device, x, y, z, w, kind, width, height) <
+               std::tie(o.device, o.x, o.y, o.z, o.w, o.kind, o.width, o.height);
+    }
+};
+std::mutex g_arr_mu;
+std::map<TexShape, std::vector<cudaArray_t>> g_arr_free;
+std::map<int, size_t> g_arr_bytes;  // kept bytes per device
+TexShape tex_shape(int dev, const cudaChannelFormatDesc& fd, size_t w, size_t h) {
+    return TexShape{dev, fd.x, fd.y, fd.z, fd.w, int(fd.f), w, h};
+}
+size_t tex_bytes(const cudaChannelFormatDesc& fd, size_t w, size_t h) {
+    return size_t(fd.x + fd.y + fd.z + fd.w) / 8 * w * h;
+}
+}  // namespace
+
+cudaError_t lux::tex_array_get(cudaArray_t* arr, const cudaChannelFormatDesc& fd, size_t width, size_t height) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    {
+        std::lock_guard<std::mutex> lk(g_arr_mu);
+        auto it = g_arr_free.find(tex_shape(dev, fd, width, height));
+        if (it != g_arr_free.end() && !it->second.empty()) {
+            *arr = it->second.back();
+            it->second.pop_back();
+            g_arr_bytes[dev] -= tex_bytes(fd, width, height);
+            return cudaSuccess;
+        }
+    }
+    e = cudaMallocArray(arr, &fd, width, height);
+    if (e == cudaSuccess) note_device_alloc();
+    return e;
+}
+
+void lux::tex_array_put(cudaArray_t arr) {
+    if (!arr) return;
+    int dev = 0;
+    cudaChannelFormatDesc fd;
+    cudaExtent ext;
+    unsigned flags = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaArrayGetInfo(&fd, &ext, &flags, arr) != cudaSuccess || flags != 0 ||
+        ext.depth != 0) {
+        cudaFreeArray(arr);
+        return;
+    }
+    const size_t bytes = tex_bytes(fd, ext.width, ext.height);
+    {
+        std::lock_guard<std::mutex> lk(g_arr_mu);
+        if (g_arr_bytes[dev] + bytes <= kTexArrayKeep) {
+            g_arr_free[tex_shape(dev, fd, ext.width, ext.height)].push_back(arr);
+            g_arr_bytes[dev] += bytes;
+            return;
+        }
+    }
+    cudaFreeArray(arr);
+}
+
+void lux::pinned_put(void* p, size_t bytes) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(g_pinned_mu);
+    g_pinned_free[pinned_class(bytes)].push_back(p);
+}
 
 extern "C" {
 
@@ -1202,8 +1301,8 @@ int lux_free(lux_ctx* C) {
     if (C->stream) cudaStreamSynchronize(C->stream);
     for (auto& g : C->graphs) cudaGraphExecDestroy(g.second);
     for (void* p : C->allocs) scratch_free(p, C->stream);
-    if (C->h_wave_iter) cudaFreeHost(C->h_wave_iter);
-    if (C->h_ctr) cudaFreeHost(C->h_ctr);
+    pinned_put(C->h_wave_iter, sizeof(int) * 2 * size_t(C->h_cap));
+    pinned_put(C->h_ctr, sizeof(WaveCounters) * size_t(C->h_cap));
     for (auto e : C->kev) cudaEventDestroy(e);
     if (C->ev[0]) cudaEventDestroy(C->ev[0]);
     if (C->ev[1]) cudaEventDestroy(C->ev[1]);

@@ -39,6 +39,15 @@ inline double ms_since(std::chrono::steady_clock::time_point t0) {
 // Counts every device allocation the library makes (lux_device_alloc_count).
 void note_device_alloc();
 
+// Small page-locked host blocks (wave counters, iteration words, build counters) from a
+// process-wide free list: cudaMallocHost and cudaFreeHost cost tens to hundreds of
+// microseconds each and synchronise, and every context and scene build needs a few such
+// blocks. A block is kept by size class (a power of two of at least 256 bytes) when put back
+// and never returned to the system. Put a block back only when no copy into or out of it is
+// still queued on any stream.
+void* pinned_get(size_t bytes);
+void pinned_put(void* p, size_t bytes);
+
 template <class T>
 int dalloc(T** p, size_t n) {
     *p = nullptr;
@@ -61,9 +70,19 @@ struct DevTex {
     cudaTextureObject_t obj = 0;
     size_t bytes = 0;
 };
+// CUDA arrays of destroyed textures are kept, per device, channel format and size, for the
+// next texture of that shape (up to kTexArrayKeep bytes per device; beyond that they are
+// freed): cudaMallocArray and cudaFreeArray synchronise the device and cost far more than the
+// copy into an array, and a renderer that reloads or replaces scenes meets the same texture
+// shapes again. tex_array_get takes a kept array or allocates one; tex_array_put keeps or
+// frees it. Put an array back only when no copy or kernel can still use it.
+constexpr size_t kTexArrayKeep = size_t(2) << 30;
+cudaError_t tex_array_get(cudaArray_t* arr, const cudaChannelFormatDesc& fd, size_t width, size_t height);
+void tex_array_put(cudaArray_t arr);
+
 inline void destroy_texture(DevTex& t) {
     if (t.obj) cudaDestroyTextureObject(t.obj);
-    if (t.arr) cudaFreeArray(t.arr);
+    if (t.arr) tex_array_put(t.arr);
     t = DevTex{};
 }
 
