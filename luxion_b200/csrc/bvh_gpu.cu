@@ -754,11 +754,27 @@ struct Item {
     int tree;
 };
 
+// The items a launch works on: [off, off + count) of the level arrays. With lvl set, both come
+// from the device level table (lvl[2 l], lvl[2 l + 1]), so that levels are launched back to back
+// without the host reading their sizes; otherwise off = 0 and count = n.
+struct Span {
+    const int* lvl;
+    int l;
+    int n;
+    __device__ int off() const { return lvl ? lvl[2 * l] : 0; }
+    __device__ int count() const { return lvl ? lvl[2 * l + 1] : n; }
+};
+
 // One 8-wide node per item: its children, slots, quantised boxes (child_base and tri_base are
 // placed later), the binary ids of its internal children and the primitives of its leaf slots,
 // both in slot order.
-__global__ void k_collapse(const Item* items, int n_items, const BinNode* bn, const int* ord_fin, BVH8Node* tmp,
-                           int* n_int, int* n_leaf, int* child_bn, int* leaf_prim) {
+__global__ void k_collapse(Span sp, const Item* items_all, const BinNode* bn, const int* ord_fin, BVH8Node* tmp_all,
+                           int* n_int_all, int* n_leaf_all, int* child_bn_all, int* leaf_prim_all) {
+    const int o = sp.off(), n_items = sp.count();
+    const Item* items = items_all + o;
+    BVH8Node* tmp = tmp_all + o;
+    int *n_int = n_int_all + o, *n_leaf = n_leaf_all + o;
+    int *child_bn = child_bn_all + size_t(o) * 8, *leaf_prim = leaf_prim_all + size_t(o) * 8;
     for (int it = blockIdx.x * blockDim.x + threadIdx.x; it < n_items; it += gridDim.x * blockDim.x) {
         const BinNode& b = bn[items[it].bnode];
         int ch[8];
@@ -890,18 +906,44 @@ __global__ void k_collapse(const Item* items, int n_items, const BinNode* bn, co
     }
 }
 
-// next level: item cs[it] + k is internal child k of item it
-__global__ void k_emit(const Item* items, int n_items, const int* n_int, const int* cs, const int* child_bn,
-                       Item* next) {
+// next level: item cs[it] + k is internal child k of item it; the next level starts right
+// after this one
+__global__ void k_emit(Span sp, Item* items_all, const int* n_int_all, const int* cs_all, const int* child_bn_all,
+                       long long cap) {
+    const int o = sp.off(), n_items = sp.count();
+    const Item* items = items_all + o;
+    const int *n_int = n_int_all + o, *cs = cs_all + o;
+    const int* child_bn = child_bn_all + size_t(o) * 8;
     for (int it = blockIdx.x * blockDim.x + threadIdx.x; it < n_items; it += gridDim.x * blockDim.x)
-        for (int k = 0; k < n_int[it]; ++k) next[cs[it] + k] = Item{child_bn[size_t(it) * 8 + k], items[it].tree};
+        for (int k = 0; k < n_int[it]; ++k) {
+            const long long at = (long long)o + n_items + cs[it] + k;  // past the capacity: k_level_next flags it
+            if (at < cap) items_all[at] = Item{child_bn[size_t(it) * 8 + k], items[it].tree};
+        }
+}
+
+// Level l + 1 of the table: it starts after level l and holds *n_next items (the total of the
+// scan of level l's internal-child counts). Past the capacity it is left empty and err is set.
+__global__ void k_level_next(int* lvl, int l, const int* n_next, long long cap, int* err) {
+    const long long o = (long long)lvl[2 * l] + lvl[2 * l + 1];
+    const int n = *n_next;
+    lvl[2 * (l + 1)] = int(o);
+    if (o + n > cap) {
+        lvl[2 * (l + 1) + 1] = 0;
+        *err = 1;
+    } else {
+        lvl[2 * (l + 1) + 1] = n;
+    }
 }
 
 // exclusive scan of n ints (in -> out), total to *total; three passes over blocks of 1024
 constexpr int kScanBlock = 1024;
-__global__ void __launch_bounds__(256) k_scan_local(const int* in, int n, int* out, int* block_sums) {
+__global__ void __launch_bounds__(256) k_scan_local(Span sp, const int* in_all, int* out_all, int* block_sums) {
     __shared__ int sh[256];
+    const int o = sp.off(), n = sp.count();
+    const int* in = in_all + o;
+    int* out = out_all + o;
     const int base = blockIdx.x * kScanBlock;
+    if (blockIdx.x > 0 && base >= n) return;  // block 0 always writes its (maybe empty) sum
     int v[4], s = 0;
     for (int k = 0; k < 4; ++k) {
         const int i = base + int(threadIdx.x) * 4 + k;
@@ -924,8 +966,9 @@ __global__ void __launch_bounds__(256) k_scan_local(const int* in, int n, int* o
     }
     if (threadIdx.x == 255) block_sums[blockIdx.x] = sh[255];
 }
-__global__ void __launch_bounds__(1024) k_scan_sums(int* block_sums, int nb, int* total) {
+__global__ void __launch_bounds__(1024) k_scan_sums(Span sp, int* block_sums, int* total) {
     __shared__ int sh[1024];
+    const int nb = max(1, (sp.count() + kScanBlock - 1) / kScanBlock);
     const int per = (nb + 1023) / 1024;
     const int b0 = min(nb, int(threadIdx.x) * per), b1 = min(nb, b0 + per);
     int s = 0;
@@ -946,7 +989,9 @@ __global__ void __launch_bounds__(1024) k_scan_sums(int* block_sums, int nb, int
     }
     if (threadIdx.x == 1023) *total = sh[1023];
 }
-__global__ void k_scan_add(int* out, int n, const int* block_sums) {
+__global__ void k_scan_add(Span sp, int* out_all, const int* block_sums) {
+    const int n = sp.count();
+    int* out = out_all + sp.off();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         out[i] += block_sums[i / kScanBlock];
 }
@@ -1258,11 +1303,13 @@ struct Bufs {
 int grid_for(int n, int per_block, int cap) { return std::max(1, std::min(cap, (n + per_block - 1) / per_block)); }
 
 // exclusive scan of n device ints (in -> out); the total lands in *total (device)
-int device_scan(const int* in, int n, int* out, int* total, int* block_sums, cudaStream_t st) {
-    const int nb = std::max(1, (n + kScanBlock - 1) / kScanBlock);
-    k_scan_local<<<nb, 256, 0, st>>>(in, n, out, block_sums);
-    k_scan_sums<<<1, 1024, 0, st>>>(block_sums, nb, total);
-    k_scan_add<<<grid_for(n, 256, 4096), 256, 0, st>>>(out, n, block_sums);
+// Exclusive scan of sp's items of in into out (both indexed from the level start); max_n bounds
+// the count for the launch shapes. The block sums need max(1, ceil(max_n / kScanBlock)) ints.
+int device_scan(Span sp, int max_n, const int* in, int* out, int* total, int* block_sums, cudaStream_t st) {
+    const int nb = std::max(1, (max_n + kScanBlock - 1) / kScanBlock);
+    k_scan_local<<<nb, 256, 0, st>>>(sp, in, out, block_sums);
+    k_scan_sums<<<1, 1024, 0, st>>>(sp, block_sums, total);
+    k_scan_add<<<grid_for(max_n, 256, 4096), 256, 0, st>>>(sp, out, block_sums);
     LUX_CUDA(cudaGetLastError());
     return LUX_OK;
 }
@@ -1394,28 +1441,67 @@ int build_bvh8_device(const float* d_boxes, const std::vector<int>& tree_begin, 
         for (int t = 0; t < G; ++t) roots[t] = Item{t, t};
         LUX_CUDA(cudaMemcpyAsync(items, roots.data(), sizeof(Item) * G, cudaMemcpyHostToDevice, st));
     }
-    std::vector<size_t> lvl_off{0};
-    std::vector<int> lvl_n{G};
-    while (true) {
-        const size_t o = lvl_off.back();
-        const int n = lvl_n.back();
-        if (o + size_t(n) > item_cap) return fail(LUX_ERR_UNSUPPORTED, "BVH build: 8-wide node capacity");
-        k_collapse<<<grid_for(n, 128, 4096), 128, 0, st>>>(items + o, n, bn, ord_fin, tmp + o, n_int + o, n_leaf + o,
-                                                          child_bn + o * 8, leafp + o * 8);
-        LUX_CUDA(cudaGetLastError());
-        if (int rc = device_scan(n_leaf + o, n, ls + o, ctr + 5, block_sums, st)) return rc;
-        if (int rc = device_scan(n_int + o, n, cs + o, ctr + 6, block_sums, st)) return rc;
-        LUX_CUDA(cudaMemcpyAsync(h_ctr, ctr, 8 * sizeof(int), cudaMemcpyDeviceToHost, st));
-        LUX_CUDA(cudaStreamSynchronize(st));
-        const int n_next = h_ctr[6];
-        if (n_next <= 0) break;
-        if (o + size_t(n) + size_t(n_next) > item_cap) return fail(LUX_ERR_UNSUPPORTED, "BVH build: 8-wide node capacity");
-        k_emit<<<grid_for(n, 128, 4096), 128, 0, st>>>(items + o, n, n_int + o, cs + o, child_bn + o * 8, items + o + n);
-        LUX_CUDA(cudaGetLastError());
-        lvl_off.push_back(o + size_t(n));
-        lvl_n.push_back(n_next);
+    // The levels are launched in batches without reading their sizes back: every kernel takes
+    // its level's offset and count from the device level table (lvl: offset, count per level;
+    // then an error word), and a level past the last is empty, so its kernels do nothing. One
+    // read-back of the table per batch finds the first empty level. The first batch covers the
+    // levels a tree of the largest size usually has (about one 8-wide level per three binary
+    // levels of a binary depth near 1.5 log2 n).
+    constexpr int kMaxLevels = 120;
+    int* lvl = B.get<int>(2 * kMaxLevels + 4);
+    int* h_lvl = static_cast<int*>(pinned_get(sizeof(int) * (2 * kMaxLevels + 4)));
+    struct LevelFree {
+        int* p;
+        cudaStream_t st;
+        ~LevelFree() {
+            cudaStreamSynchronize(st);
+            pinned_put(p, sizeof(int) * (2 * kMaxLevels + 4));
+        }
+    } lf{h_lvl, st};
+    if (!lvl || !h_lvl) return fail(LUX_ERR_OOM, "BVH build: level table allocation failed");
+    int* lvl_err = lvl + 2 * kMaxLevels + 2;
+    LUX_CUDA(cudaMemsetAsync(lvl, 0, sizeof(int) * (2 * kMaxLevels + 4), st));
+    {
+        const int first[2] = {0, G};
+        LUX_CUDA(cudaMemcpyAsync(lvl, first, sizeof(first), cudaMemcpyHostToDevice, st));
+        LUX_CUDA(cudaStreamSynchronize(st));  // `first` lives on this stack frame
     }
-    const int L = int(lvl_n.size());
+    int max_tree = 1;
+    for (int t = 0; t < G; ++t) max_tree = std::max(max_tree, tree_begin[t + 1] - tree_begin[t]);
+    const int max_n = int(item_cap);
+    const int grid_items = grid_for(max_n, 128, 148 * 16);
+    int launched = 0, L = -1;
+    int batch = int(std::ceil(0.5 * std::log2(double(max_tree) + 1.0))) + 1;
+    while (L < 0) {
+        batch = std::min(batch, kMaxLevels - launched);
+        if (batch <= 0) return fail(LUX_ERR_UNSUPPORTED, "BVH build: too many 8-wide levels");
+        for (int l = launched; l < launched + batch; ++l) {
+            const Span sp{lvl, l, 0};
+            k_collapse<<<grid_items, 128, 0, st>>>(sp, items, bn, ord_fin, tmp, n_int, n_leaf, child_bn, leafp);
+            LUX_CUDA(cudaGetLastError());
+            if (int rc = device_scan(sp, max_n, n_leaf, ls, ctr + 5, block_sums, st)) return rc;
+            if (int rc = device_scan(sp, max_n, n_int, cs, ctr + 6, block_sums, st)) return rc;
+            k_level_next<<<1, 1, 0, st>>>(lvl, l, ctr + 6, (long long)item_cap, lvl_err);
+            k_emit<<<grid_items, 128, 0, st>>>(sp, items, n_int, cs, child_bn, (long long)item_cap);
+            LUX_CUDA(cudaGetLastError());
+        }
+        launched += batch;
+        LUX_CUDA(cudaMemcpyAsync(h_lvl, lvl, sizeof(int) * (2 * kMaxLevels + 4), cudaMemcpyDeviceToHost, st));
+        LUX_CUDA(cudaStreamSynchronize(st));
+        if (h_lvl[2 * kMaxLevels + 2]) return fail(LUX_ERR_UNSUPPORTED, "BVH build: 8-wide node capacity");
+        for (int l = 1; l <= launched; ++l)
+            if (h_lvl[2 * l + 1] == 0) {
+                L = l;
+                break;
+            }
+        batch = 3;
+    }
+    std::vector<size_t> lvl_off(L);
+    std::vector<int> lvl_n(L);
+    for (int l = 0; l < L; ++l) {
+        lvl_off[l] = size_t(h_lvl[2 * l]);
+        lvl_n[l] = h_lvl[2 * l + 1];
+    }
     const size_t total_items = lvl_off.back() + size_t(lvl_n.back());
 
     // ---- placement ----

@@ -261,10 +261,13 @@ int make_texture(const lux_texture_desc& t, DevTex& out, int storage, TexStage& 
     return LUX_OK;
 }
 
-// Run fn(lo, hi) over [0, n) split into contiguous chunks, one per host thread.
+// Run fn(lo, hi) over [0, n) split into contiguous chunks, one per host thread. It runs while
+// the geometry and texture threads of a scene build launch device work, so it leaves them
+// three cores: a launching thread that waits for a core stalls the device behind it.
 template <class F>
 void parallel_chunks(int n, F fn) {
-    unsigned nt = std::max(1u, std::min(std::thread::hardware_concurrency(), 64u));
+    const unsigned hw = std::thread::hardware_concurrency();
+    unsigned nt = std::max(1u, std::min(hw > 4 ? hw - 3 : 1u, 64u));
     nt = std::max(1u, std::min(nt, unsigned((n + 63) / 64)));
     std::vector<std::thread> th;
     for (unsigned t = 1; t < nt; ++t) th.emplace_back(fn, int(int64_t(n) * t / nt), int(int64_t(n) * (t + 1) / nt));
