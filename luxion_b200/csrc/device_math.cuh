@@ -81,6 +81,15 @@ LUX_HDI uint32_t utilhash(uint32_t a) {
     a = (a ^ 0xb55a4f09u) ^ (a >> 16);
     return a;
 }
+// Path state is streamed: each kernel reads and writes a path's fields once, and a wave's
+// state (about 1.4 GB at 1080p) does not fit in L2. Evict-first loads and stores
+// (ld/st.global.cs) keep it from pushing the BVH nodes and triangle records, which every
+// traversal reads again and again, out of L2.
+LUX_DI float4 ld_stream(const float4* p) { return __ldcs(p); }
+LUX_DI int ld_stream(const int* p) { return __ldcs(p); }
+LUX_DI void st_stream(float4* p, float4 v) { __stcs(p, v); }
+LUX_DI void st_stream(int* p, int v) { __stcs(p, v); }
+
 struct Rng {
     uint32_t x;
     LUX_HDI static uint32_t mod_m(uint64_t v) {

@@ -489,10 +489,10 @@ struct PathState {
 struct WavePathIn {
     const DevWave& W;
     int pid;
-    LUX_DI f3 origin() const { float4 a = W.s0[pid]; return mk(a.x, a.y, a.z); }
-    LUX_DI float last_pdf() const { return W.s0[pid].w; }
-    LUX_DI f3 color0() const { float4 a = W.s3[pid]; return mk(a.x, a.y, a.z); }
-    LUX_DI f3 nee() const { float4 a = W.s4[pid]; return mk(a.x, a.y, a.z); }
+    LUX_DI f3 origin() const { float4 a = ld_stream(&W.s0[pid]); return mk(a.x, a.y, a.z); }
+    LUX_DI float last_pdf() const { return ld_stream(&W.s0[pid]).w; }
+    LUX_DI f3 color0() const { float4 a = ld_stream(&W.s3[pid]); return mk(a.x, a.y, a.z); }
+    LUX_DI f3 nee() const { float4 a = ld_stream(&W.s4[pid]); return mk(a.x, a.y, a.z); }
 };
 
 // shadePath for one path; returns true if the path survives (is not killed).
@@ -649,13 +649,13 @@ LUX_DI bool shade_one(const DevScene& S, const DevOptions& O, int depth, PathSta
 
 // The fields shade_one reads on entry.
 LUX_DI PathState load_path(const DevWave& W, int pid) {
-    float4 b = W.s1[pid], c = W.s2[pid];
+    float4 b = ld_stream(&W.s1[pid]), c = ld_stream(&W.s2[pid]);
     PathState p;
     p.d = mk(b.x, b.y, b.z);
     p.spec = (__float_as_int(b.w) & 1) != 0;
     p.thr = mk(c.x, c.y, c.z);
     p.pixel = __float_as_int(c.w);
-    p.iter = __float_as_int(W.s3[pid].w);
+    p.iter = __float_as_int(ld_stream(&W.s3[pid]).w);
     return p;
 }
 
@@ -673,17 +673,17 @@ __global__ void __launch_bounds__(kShadeBlock, 16) k_camera(DevScene S, DevWave 
         float pY = (float(y) + x2 + 0.5f) - float(C.height) * 0.5f;
         f3 view = ld3(C.view), right = ld3(C.right), up = ld3(C.up);
         f3 d = normalize(view - (right * C.pixel_length[0] * pX) - (up * C.pixel_length[1] * pY));
-        W.s0[pid] = make_float4(C.pos[0], C.pos[1], C.pos[2], -1.0f);
-        W.s1[pid] = make_float4(d.x, d.y, d.z, __int_as_float(0));
-        W.s2[pid] = make_float4(1.0f, 1.0f, 1.0f, __int_as_float(index));
-        W.s3[pid] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(iter));
+        st_stream(&W.s0[pid], make_float4(C.pos[0], C.pos[1], C.pos[2], -1.0f));
+        st_stream(&W.s1[pid], make_float4(d.x, d.y, d.z, __int_as_float(0)));
+        st_stream(&W.s2[pid], make_float4(1.0f, 1.0f, 1.0f, __int_as_float(index)));
+        st_stream(&W.s3[pid], make_float4(0.0f, 0.0f, 0.0f, __int_as_float(iter)));
         if (nee) {
             f3 ed;
             f3 dl = light_sample(S, O, iter, index, 0, ed, !O.env);
             f3 v = O.env ? ed : dl;
-            W.s4[pid] = make_float4(v.x, v.y, v.z, 0.0f);
+            st_stream(&W.s4[pid], make_float4(v.x, v.y, v.z, 0.0f));
         }
-        W.queue[0][pid] = pid;
+        st_stream(&W.queue[0][pid], pid);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) W.ctr->count[0] = n;
 }
@@ -710,7 +710,7 @@ __global__ void __launch_bounds__(kShadeBlock, 16) k_shade(const __grid_constant
         bool alive = false;
         int pid = 0;
         if (slot < n) {
-            pid = q[slot];
+            pid = ld_stream(&q[slot]);
             int job_compact = compact;
             const DevScene* sp = &S0;
             if (JOBS) {
@@ -720,34 +720,34 @@ __global__ void __launch_bounds__(kShadeBlock, 16) k_shade(const __grid_constant
             }
             const DevScene& S = *sp;
             PathState p = load_path(W, pid);
-            float4 h = W.hit[slot];
+            float4 h = ld_stream(&W.hit[slot]);
             int inst = __float_as_int(h.w);
-            int prim = W.hit_prim[slot];
+            int prim = ld_stream(&W.hit_prim[slot]);
             float sh_t = -1.0f, su = 0.0f, sv = 0.0f;
             int si = -1, spr = -1;
             if (nee && inst >= 0) {
-                float4 sh = W.sh_hit[slot];
+                float4 sh = ld_stream(&W.sh_hit[slot]);
                 sh_t = sh.x;
                 if (!nee_env<NEE>(O)) {
                     su = sh.y;
                     sv = sh.z;
                     si = __float_as_int(sh.w);
-                    spr = W.sh_prim[slot];
+                    spr = ld_stream(&W.sh_prim[slot]);
                 }
             }
             alive = shade_one<MATDBG, NEE, false>(S, O, depth, p, WavePathIn{W, pid}, h.x, inst, prim, h.y, h.z, sh_t, si, spr,
                                            su, sv) &&
                     job_compact;
-            W.s3[pid] = make_float4(p.color.x, p.color.y, p.color.z, __int_as_float(p.iter));
+            st_stream(&W.s3[pid], make_float4(p.color.x, p.color.y, p.color.z, __int_as_float(p.iter)));
             if (alive) {
-                W.s0[pid] = make_float4(p.o.x, p.o.y, p.o.z, p.last_pdf);
-                W.s1[pid] = make_float4(p.d.x, p.d.y, p.d.z, __int_as_float(p.spec ? 1 : 0));
-                W.s2[pid] = make_float4(p.thr.x, p.thr.y, p.thr.z, __int_as_float(p.pixel));
+                st_stream(&W.s0[pid], make_float4(p.o.x, p.o.y, p.o.z, p.last_pdf));
+                st_stream(&W.s1[pid], make_float4(p.d.x, p.d.y, p.d.z, __int_as_float(p.spec ? 1 : 0)));
+                st_stream(&W.s2[pid], make_float4(p.thr.x, p.thr.y, p.thr.z, __int_as_float(p.pixel)));
                 if (nee) {
                     f3 ed;
                     f3 dl = light_sample<NEE>(S, O, p.iter, p.pixel, depth, ed, !nee_env<NEE>(O));
                     f3 v = nee_env<NEE>(O) ? ed : dl;
-                    W.s4[pid] = make_float4(v.x, v.y, v.z, 0.0f);
+                    st_stream(&W.s4[pid], make_float4(v.x, v.y, v.z, 0.0f));
                 }
             }
         }
@@ -758,7 +758,7 @@ __global__ void __launch_bounds__(kShadeBlock, 16) k_shade(const __grid_constant
             int leader = __ffs(am) - 1;
             if (lane == leader) b = atomicAdd(&W.ctr->count[depth], __popc(am));
             b = __shfl_sync(0xffffffffu, b, leader);
-            if (alive) nq[b + __popc(am & ((1u << lane) - 1u))] = pid;
+            if (alive) st_stream(&nq[b + __popc(am & ((1u << lane) - 1u))], pid);
         }
     }
 }
@@ -771,7 +771,7 @@ __global__ void k_accumulate(const float4* __restrict__ s3, float* __restrict__ 
             // Kahan-compensated running sum (precision form)
             float cr = comp[p * 3], cg = comp[p * 3 + 1], cb = comp[p * 3 + 2];
             for (int s = 0; s < nsamples; ++s) {
-                float4 c = s3[size_t(s) * npix + p];
+                float4 c = ld_stream(&s3[size_t(s) * npix + p]);
                 float yr = c.x - cr, tr = r + yr;
                 cr = (tr - r) - yr;
                 r = tr;
@@ -787,7 +787,7 @@ __global__ void k_accumulate(const float4* __restrict__ s3, float* __restrict__ 
             comp[p * 3 + 2] = cb;
         } else {
             for (int s = 0; s < nsamples; ++s) {
-                float4 c = s3[size_t(s) * npix + p];
+                float4 c = ld_stream(&s3[size_t(s) * npix + p]);
                 r += c.x;
                 g += c.y;
                 b += c.z;

@@ -503,24 +503,24 @@ __global__ void __launch_bounds__(kTraceBlock, 7) k_trace(const __grid_constant_
                         L.pixel = __float_as_int(ry[7]);
                         L.iter = A.ext_iter;
                     } else if (MODE == 0 || MODE == 3) {
-                        int pid = A.W.queue[A.bounce & 1][r];
-                        float4 a = A.W.s0[pid], b = A.W.s1[pid];
+                        int pid = ld_stream(&A.W.queue[A.bounce & 1][r]);
+                        float4 a = ld_stream(&A.W.s0[pid]), b = ld_stream(&A.W.s1[pid]);
                         o = mk(a.x, a.y, a.z);
                         d = mk(b.x, b.y, b.z);
                         tmax = 1e16f;
-                        L.pixel = __float_as_int(A.W.s2[pid].w);
-                        L.iter = __float_as_int(A.W.s3[pid].w);
+                        L.pixel = __float_as_int(ld_stream(&A.W.s2[pid]).w);
+                        L.iter = __float_as_int(ld_stream(&A.W.s3[pid]).w);
                         if (A.W.path_job) root = A.W.jobs[A.W.path_job[pid]].tlas_root;
                     } else {
-                        int slot = A.W.sh_queue[r];
+                        int slot = ld_stream(&A.W.sh_queue[r]);
                         item = slot;
-                        float4 a = A.W.sh_o[slot], b = A.W.sh_d[slot];
+                        float4 a = ld_stream(&A.W.sh_o[slot]), b = ld_stream(&A.W.sh_d[slot]);
                         o = mk(a.x, a.y, a.z);
                         d = mk(b.x, b.y, b.z);
                         tmax = a.w;
-                        int pid = A.W.queue[A.bounce & 1][slot];
-                        L.pixel = __float_as_int(A.W.s2[pid].w);
-                        L.iter = __float_as_int(A.W.s3[pid].w);
+                        int pid = ld_stream(&A.W.queue[A.bounce & 1][slot]);
+                        L.pixel = __float_as_int(ld_stream(&A.W.s2[pid]).w);
+                        L.iter = __float_as_int(ld_stream(&A.W.s3[pid]).w);
                         if (A.W.path_job) root = A.W.jobs[A.W.path_job[pid]].tlas_root;
                     }
                     T.start(L, o, d, tmax, root);
@@ -579,8 +579,8 @@ __global__ void __launch_bounds__(kTraceBlock, 7) k_trace(const __grid_constant_
                     }
                 } else if (MODE == 0) {
                     bool hit = L.best.inst >= 0;
-                    A.W.hit[item] = make_float4(hit ? L.best.t : -1.0f, L.best.u, L.best.v, __int_as_float(L.best.inst));
-                    A.W.hit_prim[item] = L.best.prim;
+                    st_stream(&A.W.hit[item], make_float4(hit ? L.best.t : -1.0f, L.best.u, L.best.v, __int_as_float(L.best.inst)));
+                    st_stream(&A.W.hit_prim[item], L.best.prim);
                     if (hit && A.nee) {
                         // shadow ray of the raygen program (src/optixshaders/optix_triangle.cu:82-132)
                         f3 n = hit_world_normal(A.S, L.best.inst, L.best.prim, L.best.u, L.best.v);
@@ -589,8 +589,8 @@ __global__ void __launch_bounds__(kTraceBlock, 7) k_trace(const __grid_constant_
                                    __fadd_rn(wo.z, __fmul_rn(L.best.t, wd.z)));
                         f3 so = mk(__fadd_rn(hp.x, __fmul_rn(n.x, 1e-4f)), __fadd_rn(hp.y, __fmul_rn(n.y, 1e-4f)),
                                    __fadd_rn(hp.z, __fmul_rn(n.z, 1e-4f)));
-                        int pid = A.W.queue[A.bounce & 1][item];
-                        float4 ns = A.W.s4[pid];
+                        int pid = ld_stream(&A.W.queue[A.bounce & 1][item]);
+                        float4 ns = ld_stream(&A.W.s4[pid]);
                         f3 sd;
                         float tmax;
                         if (A.nee == 2) {
@@ -603,20 +603,20 @@ __global__ void __launch_bounds__(kTraceBlock, 7) k_trace(const __grid_constant_
                             sd = mk(__fmul_rn(ld.x, il), __fmul_rn(ld.y, il), __fmul_rn(ld.z, il));
                             tmax = __fadd_rn(__fmul_rn(dl, 1.0001f), 1e-4f);
                         }
-                        A.W.sh_o[item] = make_float4(so.x, so.y, so.z, tmax);
-                        A.W.sh_d[item] = make_float4(sd.x, sd.y, sd.z, 0.0f);
+                        st_stream(&A.W.sh_o[item], make_float4(so.x, so.y, so.z, tmax));
+                        st_stream(&A.W.sh_d[item], make_float4(sd.x, sd.y, sd.z, 0.0f));
                         // warp-aggregated append to the shadow queue
                         unsigned am = __activemask();
                         int leader = __ffs(am) - 1;
                         int b2 = 0;
                         if (lane == leader) b2 = atomicAdd(&A.W.ctr->shadow[A.bounce], __popc(am));
                         b2 = __shfl_sync(am, b2, leader);
-                        A.W.sh_queue[b2 + __popc(am & ((1u << lane) - 1u))] = item;
+                        st_stream(&A.W.sh_queue[b2 + __popc(am & ((1u << lane) - 1u))], item);
                     }
                 } else if (MODE == 1) {
                     bool hit = L.best.inst >= 0;
-                    A.W.sh_hit[item] = make_float4(hit ? L.best.t : -1.0f, L.best.u, L.best.v, __int_as_float(L.best.inst));
-                    A.W.sh_prim[item] = L.best.prim;
+                    st_stream(&A.W.sh_hit[item], make_float4(hit ? L.best.t : -1.0f, L.best.u, L.best.v, __int_as_float(L.best.inst)));
+                    st_stream(&A.W.sh_prim[item], L.best.prim);
                 } else if (MODE == 3) {
                     // drawBVH (src/kernels/draw_bvh.cu:33): color += count * 0.001 on every channel
                     int pid = A.W.queue[A.bounce & 1][item];
@@ -624,7 +624,7 @@ __global__ void __launch_bounds__(kTraceBlock, 7) k_trace(const __grid_constant_
                     const float h = float(L.work) * 0.001f;
                     A.W.s3[pid] = make_float4(c.x + h, c.y + h, c.z + h, c.w);
                 } else {
-                    A.W.sh_hit[item] = make_float4(L.best.inst >= 0 ? 1.0f : -1.0f, 0.0f, 0.0f, __int_as_float(-1));
+                    st_stream(&A.W.sh_hit[item], make_float4(L.best.inst >= 0 ? 1.0f : -1.0f, 0.0f, 0.0f, __int_as_float(-1)));
                 }
             }
             const unsigned am = __ballot_sync(FULL, active);
