@@ -27,9 +27,12 @@
 namespace lux {
 namespace {
 
+// A closest hit as the shading reads it. The tangent frame is only read under a normal map,
+// so it is rebuilt there from the hit (hit_tangent) instead of for every hit.
 struct Isect {
     float t;
-    f3 normal, tangent;
+    f3 normal;
+    int inst, prim;
     int material;
     float u, v;
 };
@@ -56,27 +59,51 @@ LUX_DI void mesh_tri(const DevScene& S, const DevInstance& I, int prim, uint32_t
     i2 = I.vert_base + __ldg(id + 2);
 }
 
-// closest-hit program (src/optixshaders/optix_triangle.cu:156-243)
+// closest-hit program (src/optixshaders/optix_triangle.cu:156-243); its tangent is hit_tangent
 LUX_DI Isect ch_radiance(const DevScene& S, float t, int inst, int prim, float bu, float bv) {
     Isect r;
     const DevInstance& I = S.insts[inst];
     uint32_t i0, i1, i2;
     mesh_tri(S, I, prim, i0, i1, i2);
-    f3 A = ld3(S.pos + i0 * 3), B = ld3(S.pos + i1 * 3), C = ld3(S.pos + i2 * 3);
-    f3 e1 = B - A, e2 = C - A;
-    f3 n = normalize(cross(e1, e2));
+    f3 n;
     float bA = 1.0f - bu - bv;
     if (I.flags & kInstHasNormals) {
         f3 nA = ld3(S.nrm + i0 * 3), nB = ld3(S.nrm + i1 * 3), nC = ld3(S.nrm + i2 * 3);
         n = normalize(bA * nA + bu * nB + bv * nC);
+    } else {
+        f3 A = ld3(S.pos + i0 * 3), B = ld3(S.pos + i1 * 3), C = ld3(S.pos + i2 * 3);
+        n = normalize(cross(B - A, C - A));
     }
-    f3 tg = mk(1.0f, 0.0f, 0.0f);
     float uu = 0.0f, vv = 0.0f;
     if (I.flags & kInstHasUVs) {
         float ax = S.uv[i0 * 2], ay = S.uv[i0 * 2 + 1], bx = S.uv[i1 * 2], by = S.uv[i1 * 2 + 1];
         float cx = S.uv[i2 * 2], cy = S.uv[i2 * 2 + 1];
         uu = bA * ax + bu * bx + bv * cx;
         vv = bA * ay + bu * by + bv * cy;
+    }
+    r.t = t;
+    r.normal = normalize(xform(I.MinvT, n, 0.0f));
+    r.inst = inst;
+    r.prim = prim;
+    r.material = I.material;
+    r.u = uu;
+    r.v = vv;
+    return r;
+}
+
+// The closest-hit program's world tangent (optix_triangle.cu:194-223): the object-space
+// tangent from the uv deltas, transformed by the instance, then made orthogonal to the world
+// normal n (the hit's is.normal).
+LUX_DI f3 hit_tangent(const DevScene& S, int inst, int prim, f3 n) {
+    const DevInstance& I = S.insts[inst];
+    uint32_t i0, i1, i2;
+    mesh_tri(S, I, prim, i0, i1, i2);
+    f3 tg = mk(1.0f, 0.0f, 0.0f);
+    if (I.flags & kInstHasUVs) {
+        f3 A = ld3(S.pos + i0 * 3), B = ld3(S.pos + i1 * 3), C = ld3(S.pos + i2 * 3);
+        f3 e1 = B - A, e2 = C - A;
+        float ax = S.uv[i0 * 2], ay = S.uv[i0 * 2 + 1], bx = S.uv[i1 * 2], by = S.uv[i1 * 2 + 1];
+        float cx = S.uv[i2 * 2], cy = S.uv[i2 * 2 + 1];
         float d1x = bx - ax, d1y = by - ay, d2x = cx - ax, d2y = cy - ay;
         float det = d1x * d2y - d2x * d1y;
         float f = (fabsf(det) < 1e-10f) ? 0.0f : 1.0f / det;
@@ -86,7 +113,6 @@ LUX_DI Isect ch_radiance(const DevScene& S, float t, int inst, int prim, float b
             tg.z = f * (d2y * e1.z - d1y * e2.z);
         }
     }
-    n = normalize(xform(I.MinvT, n, 0.0f));
     tg = normalize(xform(I.M, tg, 0.0f));
     f3 T = tg - dot(tg, n) * n;
     float l2 = dot(T, T);
@@ -96,13 +122,7 @@ LUX_DI Isect ch_radiance(const DevScene& S, float t, int inst, int prim, float b
         tg = (fabsf(n.x) > 0.9f) ? mk(0.0f, 1.0f, 0.0f) : mk(1.0f, 0.0f, 0.0f);
         tg = normalize(cross(tg, n));
     }
-    r.t = t;
-    r.normal = n;
-    r.tangent = tg;
-    r.material = I.material;
-    r.u = uu;
-    r.v = vv;
-    return r;
+    return tg;
 }
 
 // direct-light closest-hit program (src/optixshaders/optix_triangle.cu:259-305)
@@ -126,7 +146,8 @@ LUX_DI Isect ch_direct_light(const DevScene& S, float t, int inst, int prim, flo
     }
     r.t = t;
     r.normal = normalize(xform(I.MinvT, n, 0.0f));
-    r.tangent = mk(0.0f, 0.0f, 0.0f);
+    r.inst = inst;
+    r.prim = prim;
     r.material = I.material;
     r.u = uu;
     r.v = vv;
@@ -142,7 +163,7 @@ LUX_DI f3 get_albedo(const DevMaterial& m, float u, float v) {
     }
     return mk(m.color[0], m.color[1], m.color[2]);
 }
-LUX_DI f3 get_normal(const DevMaterial& m, const Isect& is) {
+LUX_DI f3 get_normal(const DevScene& S, const DevMaterial& m, const Isect& is) {
     if (m.flags & kMatNormalTex) {
         float u = is.u, v = is.v;
         tt_apply(m.normal_tt, u, v);
@@ -150,7 +171,8 @@ LUX_DI f3 get_normal(const DevMaterial& m, const Isect& is) {
         f3 ln = mk(t.x * 2.0f - 1.0f, t.y * 2.0f - 1.0f, t.z * 2.0f - 1.0f);
         const f3 N = is.normal;
         if (!(dot(ln, ln) > 1e-12f)) return N;
-        f3 T = is.tangent - dot(is.tangent, N) * N;
+        const f3 tangent = hit_tangent(S, is.inst, is.prim, N);
+        f3 T = tangent - dot(tangent, N) * N;
         float t2 = dot(T, T);
         if (!(t2 > 1e-12f)) return N;
         T = T * (1.0f / sqrtf(t2));
@@ -516,7 +538,7 @@ LUX_DI bool shade_one(const DevScene& S, const DevOptions& O, int depth, PathSta
         Isect is = ch_radiance(S, t, inst, prim, bu, bv);
         const DevMaterial& m = S.mats[is.material];
         f3 mc = get_albedo(m, is.u, is.v);
-        f3 normal = get_normal(m, is);
+        f3 normal = get_normal(S, m, is);
         float rough, metal;
         get_mr(m, is.u, is.v, rough, metal);
         if (MATDBG && O.material_debug) {
