@@ -99,6 +99,12 @@ struct lux_scene {
     }
 };
 
+// Waves of one render call whose first iteration and size the device table holds; a longer
+// call runs in chunks of this many waves.
+constexpr int kWaveTab = 4096;
+// Lanes (waves in flight) of a pipelined render call.
+constexpr int kMaxLanes = lux::kMaxSegs;
+
 struct lux_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -122,8 +128,20 @@ struct lux_ctx {
     int* h_wave_iter = nullptr;          // pinned, two ints per wave of the current call
     WaveCounters* h_ctr = nullptr;       // pinned, one per wave of the current call
     int h_cap = 0;
-    // graphs per wave size
+    // lanes of the wave arrays (waves in flight at once) and the lane of the last wave rendered
+    int lanes = 1;
+    int last_lane = 0;
+    void* wave_block = nullptr;  // the wave arrays' allocation (one of allocs)
+    // graphs: per wave size (one wave at a time), and per (waves, last wave size) of a
+    // pipelined call; both hold device and page-locked host pointers of this context
     std::map<int, cudaGraphExec_t> graphs;
+    std::map<std::pair<int, int>, cudaGraphExec_t> pgraphs;  // (waves, last wave size)
+    void drop_graphs() {
+        for (auto& g : graphs) cudaGraphExecDestroy(g.second);
+        graphs.clear();
+        for (auto& g : pgraphs) cudaGraphExecDestroy(g.second);
+        pgraphs.clear();
+    }
     // stats of the last call
     lux_stats stats{};
     bool timing = false;
@@ -672,10 +690,20 @@ int scene_create(const lux_scene_desc& d, const lux_options& o, const std::funct
 
 // The wave's arrays are carved from one allocation (each 256-byte aligned), so that a
 // context costs one cudaMalloc and one cudaFree for its whole path state.
-int alloc_wave(lux_ctx* C, int max_paths) {
+// Wave arrays for `lanes` waves of max_paths paths each (lane l: paths and slots
+// [l * max_paths, (l + 1) * max_paths)), counters per lane, and the table of the waves of a
+// render call. Replaces an earlier allocation (the graphs captured on it are dropped).
+int alloc_wave(lux_ctx* C, int max_paths, int lanes) {
     DevWave& W = C->W;
+    if (C->wave_block) {
+        if (C->stream) cudaStreamSynchronize(C->stream);
+        C->drop_graphs();
+        scratch_free(C->wave_block, C->stream);
+        C->allocs.erase(std::remove(C->allocs.begin(), C->allocs.end(), C->wave_block), C->allocs.end());
+        C->wave_block = nullptr;
+    }
     std::memset(&W, 0, sizeof(W));
-    const size_t n = size_t(max_paths);
+    const size_t n1 = size_t(max_paths), n = n1 * size_t(lanes);
     size_t off = 0;
     std::vector<std::pair<void**, size_t>> parts;
     auto take = [&](auto*& p, size_t count) {
@@ -697,24 +725,28 @@ int alloc_wave(lux_ctx* C, int max_paths) {
     take(W.sh_queue, n);
     take(W.sh_hit, n);
     take(W.sh_prim, n);
-    take(W.ctr, 1);
-    take(W.wave_iter, 4);
+    take(W.ctr, size_t(lanes));
+    take(W.wave_iter, 2 * size_t(kWaveTab));
     char* sort_temp = nullptr;
-    if (C->opt.ray_sorting) {
-        take(W.keys, n);
-        take(W.keys_alt, n);
-        take(W.queue_alt, n);
+    if (C->opt.ray_sorting) {  // ray sorting runs one wave at a time, in lane 0
+        take(W.keys, n1);
+        take(W.keys_alt, n1);
+        take(W.queue_alt, n1);
         C->sort_temp_bytes = morton_sort_temp_bytes(max_paths);
         take(sort_temp, C->sort_temp_bytes);
     }
     char* base = nullptr;
     if (int rc = C->alloc(&base, off)) return rc;
+    C->wave_block = base;
     for (auto& pt : parts) *pt.first = base + pt.second;
     if (C->opt.ray_sorting) C->sort_temp = sort_temp;
     W.npix = C->npix;
     W.width = C->width;
     W.height = C->height;
     W.max_paths = max_paths;
+    W.lane_stride = max_paths;
+    C->lanes = lanes;
+    C->last_lane = 0;
     return LUX_OK;
 }
 
@@ -732,7 +764,7 @@ int enqueue_wave(lux_ctx* C, int ns, const cudaEvent_t* ev) {
     };
     LUX_CUDA(cudaMemsetAsync(W.ctr, 0, sizeof(WaveCounters), st));
     rec();
-    LUX_CUDA(launch_camera(C->S, W, C->dopt, C->cam, n, st));
+    LUX_CUDA(launch_camera(C->S, W, C->dopt, C->cam, n, 0, W.wave_iter, st));
     rec();
     for (int b = 0; b < depth; ++b) {
         if (C->opt.ray_sorting) LUX_CUDA(launch_morton_sort(C->S, W, b, C->sort_temp, C->sort_temp_bytes, st));
@@ -750,12 +782,186 @@ int enqueue_wave(lux_ctx* C, int ns, const cudaEvent_t* ev) {
         LUX_CUDA(launch_shade(C->S, W, C->dopt, b, (b + 1) < depth ? 1 : 0, st));
         rec();
     }
-    LUX_CUDA(launch_accumulate(W, C->image, C->comp, ns, C->opt.precision == LUX_PRECISION_COMPENSATED, st));
+    LUX_CUDA(launch_accumulate(W, 0, C->image, C->comp, ns, C->opt.precision == LUX_PRECISION_COMPENSATED, st));
     rec();
     return LUX_OK;
 }
 
 int events_needed(const lux_ctx* C) { return 3 + 3 * C->dopt.trace_depth; }
+
+// ---- pipelined waves ------------------------------------------------------------------------
+// After the first bounces almost every path of a wave has ended (Russian roulette), but each
+// of its remaining bounces still costs a full launch of traversal, occlusion and shading whose
+// time is the latency of a few rays. Several waves are therefore kept in flight, one per lane:
+// wave w starts at step w * P and runs bounce t - w * P at step t, and every step is one set of
+// launches over all waves in flight (launch_trace_segs / launch_shade_segs). With L lanes and
+// P = ceil(depth / L), lane w % L is free again when wave w starts. Every path is computed as in
+// the one-wave schedule, waves end in order and each is accumulated as it ends, in sample
+// order, so the image is the same bit for bit.
+int lanes_wanted(const lux_ctx* C) {
+    const int depth = C->dopt.trace_depth;
+    if (C->opt.ray_sorting || C->opt.debug_bvh || depth < 2) return 1;
+    return std::min(kMaxLanes, depth);
+}
+
+// Events of a timed call: (event, what the interval that it ends measured).
+enum { kSpanNone = 0, kSpanCamera, kSpanTrace, kSpanShade, kSpanAccum };
+struct Spans {
+    lux_ctx* C;
+    std::vector<std::pair<int, int>> marks;
+    int mark(int what) {
+        if (!C->timing) return LUX_OK;
+        const size_t i = marks.size();
+        if (i >= C->kev.size()) {
+            C->kev.emplace_back();
+            LUX_CUDA(cudaEventCreate(&C->kev.back()));
+        }
+        LUX_CUDA(cudaEventRecord(C->kev[i], C->stream));
+        marks.emplace_back(int(i), what);
+        return LUX_OK;
+    }
+};
+
+// Waves [0, nw) of the call (table entries of W.wave_iter), the last one of ns_last samples;
+// counters of wave w are copied to h_ctr[h0 + w] when it ends.
+int enqueue_pipelined(lux_ctx* C, int nw, int ns_last, int h0, Spans* sp) {
+    cudaStream_t st = C->stream;
+    DevWave& W = C->W;
+    const int D = C->dopt.trace_depth, L = C->lanes, P = (D + L - 1) / L;
+    const int nee = C->dopt.env ? 2 : (C->dopt.dl ? 1 : 0);
+    const int steps = (nw - 1) * P + D;
+    auto ns_of = [&](int w) { return w == nw - 1 ? ns_last : C->spp_per_wave; };
+    if (sp) if (int rc_ = sp->mark(kSpanNone)) return rc_;
+    for (int t = 0; t < steps; ++t) {
+        if (t % P == 0 && t / P < nw) {
+            const int w = t / P, lane = w % L;
+            LUX_CUDA(cudaMemsetAsync(W.ctr + lane, 0, sizeof(WaveCounters), st));
+            LUX_CUDA(launch_camera(C->S, W, C->dopt, C->cam, ns_of(w) * C->npix, lane, W.wave_iter + 2 * w, st));
+            if (sp) if (int rc_ = sp->mark(kSpanCamera)) return rc_;
+        }
+        Segs G{};
+        const int w_lo = std::max(0, (t - D) / P), w_hi = std::min(nw - 1, t / P);
+        for (int w = w_lo; w <= w_hi; ++w) {
+            const int b = t - w * P;
+            if (b < 0 || b >= D) continue;
+            if (G.n == kMaxSegs) return fail(LUX_ERR_STATE, "wave schedule: too many waves in flight");
+            G.lane[G.n] = w % L;
+            G.bounce[G.n] = b;
+            G.compact[G.n] = (b + 1) < D ? 1 : 0;
+            ++G.n;
+        }
+        LUX_CUDA(launch_trace_segs(C->S, W, G, 0, nee, st));
+        if (nee) LUX_CUDA(launch_trace_segs(C->S, W, G, nee == 2 ? 2 : 1, 0, st));
+        if (sp) if (int rc_ = sp->mark(kSpanTrace)) return rc_;
+        LUX_CUDA(launch_shade_segs(C->S, W, C->dopt, G, st));
+        if (sp) if (int rc_ = sp->mark(kSpanShade)) return rc_;
+        // the wave that ran its last bounce: counters out, then its samples into the image
+        const int we = t - (D - 1);
+        if (we >= 0 && we % P == 0 && we / P < nw) {
+            const int w = we / P, lane = w % L;
+            LUX_CUDA(cudaMemcpyAsync(&C->h_ctr[h0 + w], W.ctr + lane, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st));
+            LUX_CUDA(launch_accumulate(W, lane, C->image, C->comp, ns_of(w),
+                                       C->opt.precision == LUX_PRECISION_COMPENSATED, st));
+            if (sp) if (int rc_ = sp->mark(kSpanAccum)) return rc_;
+            C->last_lane = lane;
+        }
+    }
+    return LUX_OK;
+}
+
+// Stats of a finished call from the waves' counters and, when timed, the marked spans.
+int finish_stats(lux_ctx* C, int nwaves, int n_iter, const Spans* sp, int steps) {
+    const int depth = C->dopt.trace_depth;
+    const bool nee = C->dopt.dl || C->dopt.env;
+    const int spw = C->spp_per_wave;
+    for (int w = 0; w < nwaves; ++w) {
+        const WaveCounters& c = C->h_ctr[w];
+        if (c.error) return fail(LUX_ERR_UNSUPPORTED, "traversal stack overflow");
+        for (int b = 0; b < depth; ++b) {
+            C->stats.rays_radiance += c.count[b];
+            C->stats.path_bounces += c.count[b];
+            C->stats.rays_shadow += c.shadow[b];
+        }
+        const int ns = std::min(spw, n_iter - w * spw);
+        C->stats.samples += double(ns) * C->npix;
+    }
+    C->stats.launches_camera += nwaves;
+    C->stats.launches_accum += nwaves;
+    C->stats.launches_trace += steps * (nee ? 2 : 1);
+    C->stats.launches_shade += steps;
+    if (sp) {
+        for (size_t i = 1; i < sp->marks.size(); ++i) {
+            float t = 0.0f;
+            cudaEventElapsedTime(&t, C->kev[sp->marks[i - 1].first], C->kev[sp->marks[i].first]);
+            switch (sp->marks[i].second) {
+                case kSpanCamera: C->stats.ms_camera += t; break;
+                case kSpanTrace: C->stats.ms_trace += t; break;
+                case kSpanShade: C->stats.ms_shade += t; break;
+                case kSpanAccum: C->stats.ms_accum += t; break;
+                default: break;
+            }
+        }
+    }
+    C->stats.kernel_launches = C->stats.launches_camera + C->stats.launches_accum + C->stats.launches_trace +
+                               C->stats.launches_shade + C->stats.launches_sort;
+    return LUX_OK;
+}
+
+// A render call of several waves with `lanes` of them in flight (enqueue_pipelined).
+int run_pipelined(lux_ctx* C, int first_iter, int n_iter, int nwaves, int lanes) {
+    cudaStream_t st = C->stream;
+    const int spw = C->spp_per_wave;
+    if (C->lanes < lanes)
+        if (int rc = alloc_wave(C, spw * C->npix, lanes)) return rc;
+    const int D = C->dopt.trace_depth, P = (D + C->lanes - 1) / C->lanes;
+    std::memset(&C->stats, 0, sizeof(C->stats));
+    Spans spans{C, {}};
+    LUX_CUDA(cudaEventRecord(C->ev[0], st));
+    int steps = 0;
+    for (int c0 = 0; c0 < nwaves; c0 += kWaveTab) {
+        const int nw = std::min(kWaveTab, nwaves - c0);
+        int ns_last = 0;
+        for (int w = 0; w < nw; ++w) {
+            const int it0 = first_iter + (c0 + w) * spw;
+            ns_last = std::min(spw, first_iter + n_iter - it0);
+            C->h_wave_iter[2 * (c0 + w)] = it0;
+            C->h_wave_iter[2 * (c0 + w) + 1] = ns_last;
+        }
+        LUX_CUDA(cudaMemcpyAsync(C->W.wave_iter, &C->h_wave_iter[2 * c0], 2 * sizeof(int) * size_t(nw),
+                                 cudaMemcpyHostToDevice, st));
+        if (C->opt.use_graph && !C->timing) {
+            // the graph bakes in the chunk's counter copies (h_ctr + c0) and its wave count
+            const std::pair<int, int> key{(c0 / kWaveTab) * (kWaveTab + 1) + nw, ns_last};
+            auto it = C->pgraphs.find(key);
+            if (it == C->pgraphs.end()) {
+                cudaGraph_t g;
+                LUX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                int rc = enqueue_pipelined(C, nw, ns_last, c0, nullptr);
+                cudaError_t ce = cudaStreamEndCapture(st, &g);
+                if (rc) return rc;
+                if (ce != cudaSuccess) return fail(LUX_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+                cudaGraphExec_t ge;
+                cudaError_t ie = cudaGraphInstantiate(&ge, g, 0);
+                cudaGraphDestroy(g);
+                if (ie != cudaSuccess) return fail(LUX_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+                it = C->pgraphs.emplace(key, ge).first;
+            }
+            LUX_CUDA(cudaGraphLaunch(it->second, st));
+        } else {
+            if (int rc = enqueue_pipelined(C, nw, ns_last, c0, C->timing ? &spans : nullptr)) return rc;
+        }
+        steps += (nw - 1) * P + D;
+        C->last_lane = (nw - 1) % C->lanes;
+    }
+    LUX_CUDA(cudaEventRecord(C->ev[1], st));
+    LUX_CUDA(cudaEventSynchronize(C->ev[1]));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, C->ev[0], C->ev[1]);
+    C->stats.ms_total = ms;
+    if (int rc = finish_stats(C, nwaves, n_iter, C->timing ? &spans : nullptr, steps)) return rc;
+    C->accumulated += n_iter;
+    return LUX_OK;
+}
 
 int run_waves(lux_ctx* C, int first_iter, int n_iter) {
     if (n_iter <= 0) return LUX_OK;
@@ -763,7 +969,9 @@ int run_waves(lux_ctx* C, int first_iter, int n_iter) {
     const int spw = C->spp_per_wave;
     const int nwaves = (n_iter + spw - 1) / spw;
     if (C->h_cap < nwaves) {
-        // the previous call ended with a synchronize, so no copy uses the old blocks
+        // the previous call ended with a synchronize, so no copy uses the old blocks; graphs
+        // of pipelined calls copy counters into them, so they go too
+        C->drop_graphs();
         pinned_put(C->h_ctr, sizeof(WaveCounters) * size_t(C->h_cap));
         pinned_put(C->h_wave_iter, sizeof(int) * 2 * size_t(C->h_cap));
         C->h_ctr = nullptr;
@@ -774,6 +982,9 @@ int run_waves(lux_ctx* C, int first_iter, int n_iter) {
         if (!C->h_ctr || !C->h_wave_iter) return fail(LUX_ERR_OOM, "page-locked host allocation failed");
         C->h_cap = nwaves;
     }
+    const int want = lanes_wanted(C);
+    if (want > 1 && nwaves > 1) return run_pipelined(C, first_iter, n_iter, nwaves, want);
+    C->last_lane = 0;
     const int epw = events_needed(C);
     if (C->timing && int(C->kev.size()) < epw * nwaves) {
         size_t have = C->kev.size();
@@ -1084,7 +1295,7 @@ int ctx_prepare(const lux_options& o, const lux_camera_desc& cd, int scene_depth
 // Per-pixel and per-path device memory of a context (the part pathtraceInit allocates,
 // src/pathtrace/pathtrace_buffers.cu:21-140).
 int ctx_alloc(lux_ctx* C) {
-    int r = alloc_wave(C, C->spp_per_wave * C->npix);
+    int r = alloc_wave(C, C->spp_per_wave * C->npix, 1);
     if (!r) r = C->alloc(&C->image, size_t(C->npix) * 3);
     if (!r && C->opt.precision == LUX_PRECISION_COMPENSATED) r = C->alloc(&C->comp, size_t(C->npix) * 3);
     if (!r) r = C->alloc(&C->rgba, size_t(C->npix) * 4);
@@ -1293,8 +1504,7 @@ int lux_set_camera(lux_ctx* C, const lux_camera_desc* cd) {
     C->cam.pixel_length[0] = cd->pixel_length[0];
     C->cam.pixel_length[1] = cd->pixel_length[1];
     // camera parameters are baked into captured graphs
-    for (auto& g : C->graphs) cudaGraphExecDestroy(g.second);
-    C->graphs.clear();
+    C->drop_graphs();
     return lux_reset(C);
 }
 
@@ -1302,7 +1512,7 @@ int lux_free(lux_ctx* C) {
     if (!C) return LUX_OK;
     cudaSetDevice(C->device);
     if (C->stream) cudaStreamSynchronize(C->stream);
-    for (auto& g : C->graphs) cudaGraphExecDestroy(g.second);
+    C->drop_graphs();
     for (void* p : C->allocs) scratch_free(p, C->stream);
     pinned_put(C->h_wave_iter, sizeof(int) * 2 * size_t(C->h_cap));
     pinned_put(C->h_ctr, sizeof(WaveCounters) * size_t(C->h_cap));
@@ -1332,7 +1542,7 @@ int lux_wave_counts(lux_ctx* C, int* paths, int* shadow, int max_bounces) {
     if (!C || !paths || !shadow || max_bounces < 0) return fail(LUX_ERR_INVALID, "bad arguments");
     LUX_CUDA(cudaSetDevice(C->device));
     WaveCounters hc;
-    LUX_CUDA(cudaMemcpyAsync(&hc, C->W.ctr, sizeof(hc), cudaMemcpyDeviceToHost, C->stream));
+    LUX_CUDA(cudaMemcpyAsync(&hc, C->W.ctr + C->last_lane, sizeof(hc), cudaMemcpyDeviceToHost, C->stream));
     LUX_CUDA(cudaStreamSynchronize(C->stream));
     const int n = std::min(max_bounces, kMaxDepth);
     for (int b = 0; b < n; ++b) {

@@ -159,6 +159,27 @@ struct DevSegment {
 };
 constexpr int kMaxSegments = 256;
 
+// Waves in flight together (wave pipelining). A wave lives in a lane: lane l owns paths and
+// slots [l * lane_stride, (l + 1) * lane_stride) of every per-path and per-slot array (state,
+// queues, hit and shadow records) and the counters ctr[l]. Path ids and slots are absolute, so
+// a kernel finds a lane's data at its offset. One bounce-step launch covers up to kMaxSegs
+// segments, each a lane at its own bounce; the single-wave paths use one segment, lane 0.
+constexpr int kMaxSegs = 4;
+struct Segs {
+    int n;                  // segments, 1 .. kMaxSegs
+    int lane[kMaxSegs];
+    int bounce[kMaxSegs];   // the lane's bounce (depth after shading = bounce + 1)
+    int compact[kMaxSegs];  // shade: append survivors to the lane's next queue
+};
+inline Segs one_seg(int bounce, int compact = 1) {
+    Segs g{};
+    g.n = 1;
+    g.lane[0] = 0;
+    g.bounce[0] = bounce;
+    g.compact[0] = compact;
+    return g;
+}
+
 struct DevWave {
     float4* s0;
     float4* s1;
@@ -176,8 +197,8 @@ struct DevWave {
     uint32_t* keys;   // Morton keys (ray sorting)
     uint32_t* keys_alt;
     int* queue_alt;
-    WaveCounters* ctr;
-    int* wave_iter;   // [0] first iteration of the wave, [1] samples in the wave
+    WaveCounters* ctr;  // one per lane
+    int* wave_iter;   // per wave of a render call: first iteration, samples
     // job engine only (null for a single-job context):
     const DevScene* scenes;    // per resident scene: geometry of the concatenated arrays + its lights
     const DevJob* jobs;
@@ -186,7 +207,8 @@ struct DevWave {
     int* path_job;             // job of each path
     int npix;         // pixels of the job
     int width, height;
-    int max_paths;
+    int max_paths;    // paths of one lane
+    int lane_stride;  // paths (and slots) per lane; lanes = allocated / lane_stride
 };
 
 }  // namespace lux

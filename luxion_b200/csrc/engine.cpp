@@ -339,6 +339,7 @@ int lux_engine_create(const lux_scene_desc* const* scenes, int num_scenes, const
     W.jobs = E->jobs_d;
     W.segs = E->segs_d;
     W.max_paths = E->paths_alloc;
+    W.lane_stride = E->paths_alloc;  // one lane
     if (cudaMallocHost(&E->jobs_h, sizeof(DevJob) * E->max_jobs) != cudaSuccess ||
         cudaMallocHost(&E->segs_h, sizeof(DevSegment) * kMaxSegments) != cudaSuccess ||
         cudaMallocHost(&E->hdr_h, sizeof(int) * 4) != cudaSuccess ||

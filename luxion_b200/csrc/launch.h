@@ -18,6 +18,9 @@ int shade_grid_blocks();
 // grid > 0 overrides the persistent grid (blocks), for the job engine's autotuner
 cudaError_t launch_trace(const DevScene& S, const DevWave& W, int bounce, int mode, int nee, cudaStream_t st,
                          int grid = 0);
+// the same over several (lane, bounce) segments of waves in flight, in one launch
+cudaError_t launch_trace_segs(const DevScene& S, const DevWave& W, const Segs& G, int mode, int nee, cudaStream_t st,
+                              int grid = 0);
 // trace caller rays (device buffers), n * 8 floats -> n * 5 words; fetch is a zeroed int
 cudaError_t launch_trace_ext(const DevScene& S, const DevWave& W, const float* rays, uint32_t* hits, int n, int mode,
                              int iter, int* fetch, cudaStream_t st);
@@ -32,18 +35,22 @@ struct TraceScratch {
 cudaError_t trace_static_scratch(int device, TraceScratch& out);
 size_t trace_static_scratch_bytes();
 
-// camera rays for paths [0, n) of the wave (+ NEE sample of bounce 0), queue 0 = identity
+// camera rays for paths [0, n) of a wave in lane `lane` (+ NEE sample of bounce 0), queue 0 =
+// identity; wave_iter: the wave's first iteration and sample count (device)
 cudaError_t launch_camera(const DevScene& S, const DevWave& W, const DevOptions& O, const DevCamera& cam, int n,
-                          cudaStream_t st);
+                          int lane, const int* wave_iter, cudaStream_t st);
 // shade bounce `bounce` (depth = bounce + 1 after the increment of src/pathtrace.cu:264)
 cudaError_t launch_shade(const DevScene& S, const DevWave& W, const DevOptions& O, int bounce, int compact,
                          cudaStream_t st);
+// the same over several (lane, bounce) segments of waves in flight, in one launch
+cudaError_t launch_shade_segs(const DevScene& S, const DevWave& W, const DevOptions& O, const Segs& G,
+                              cudaStream_t st);
 // job engine: camera rays of the wave's segments (counts read from W.wave_hdr), and the
 // per-job accumulation of the segments in sample order
 cudaError_t launch_camera_jobs(const DevWave& W, const DevOptions& O, int max_paths, cudaStream_t st);
 cudaError_t launch_accumulate_jobs(const DevWave& W, int compensated, cudaStream_t st);
-// image[p] (+comp) += radiance of every sample of the wave, in sample order
-cudaError_t launch_accumulate(const DevWave& W, float* image, float* comp, int nsamples, int compensated,
+// image[p] (+comp) += radiance of every sample of the wave in lane `lane`, in sample order
+cudaError_t launch_accumulate(const DevWave& W, int lane, float* image, float* comp, int nsamples, int compensated,
                               cudaStream_t st);
 cudaError_t launch_tonemap(const float* image, uint8_t* rgba, int npix, float iter, int color_mode, cudaStream_t st);
 

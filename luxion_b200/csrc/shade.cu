@@ -681,11 +681,15 @@ LUX_DI PathState load_path(const DevWave& W, int pid) {
     return p;
 }
 
-__global__ void __launch_bounds__(kShadeBlock, 16) k_camera(DevScene S, DevWave W, DevOptions O, DevCamera C, int n) {
-    const int first_iter = W.wave_iter[0];
+// Paths [0, n) of a wave in lane `lane`: path ids and queue slots from lane * lane_stride on.
+__global__ void __launch_bounds__(kShadeBlock, 16) k_camera(DevScene S, DevWave W, DevOptions O, DevCamera C, int n,
+                                                            int lane, const int* wave_iter) {
+    const int first_iter = wave_iter[0];
     const bool nee = O.dl || O.env;
-    for (int pid = blockIdx.x * blockDim.x + threadIdx.x; pid < n; pid += gridDim.x * blockDim.x) {
-        int s = pid / W.npix, index = pid - s * W.npix;
+    const int base = lane * W.lane_stride;
+    for (int local = blockIdx.x * blockDim.x + threadIdx.x; local < n; local += gridDim.x * blockDim.x) {
+        const int pid = base + local;
+        int s = local / W.npix, index = local - s * W.npix;
         int iter = first_iter + s;
         int x = index % C.width, y = index / C.width;
         Rng rng = Rng::seeded(iter, index, O.trace_depth);
@@ -707,7 +711,7 @@ __global__ void __launch_bounds__(kShadeBlock, 16) k_camera(DevScene S, DevWave 
         }
         st_stream(&W.queue[0][pid], pid);
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) W.ctr->count[0] = n;
+    if (blockIdx.x == 0 && threadIdx.x == 0) (W.ctr + lane)->count[0] = n;
 }
 
 // JOBS: the shared wavefront of the job engine; each path shades against its job's scene
@@ -716,24 +720,36 @@ __global__ void __launch_bounds__(kShadeBlock, 16) k_camera(DevScene S, DevWave 
 // texture fetches and gathers, and hiding that latency with more warps pays more than the
 // register spills cost (shade per 16-spp step of the 1M-triangle 1080p workload: 28.3 ms at
 // 5 blocks per SM, 22.6 at 8, 20.4 at 12, 18.8 at 16).
+// G: the (lane, bounce) segments of waves in flight this launch shades; the paths of segment k
+// are its lane's queue at its bounce, and its survivors go to the lane's next queue.
 template <bool JOBS, bool MATDBG, int NEE>
 __global__ void __launch_bounds__(kShadeBlock, 16) k_shade(const __grid_constant__ DevScene S0, DevWave W, DevOptions O,
-                                                       int bounce, int compact) {
-    const int n = *(volatile int*)&W.ctr->count[bounce];
-    const int depth = bounce + 1;
-    const int* q = W.queue[bounce & 1];
-    int* nq = W.queue[(bounce + 1) & 1];
+                                                       const __grid_constant__ Segs G) {
+    __shared__ int seg_first[kMaxSegs + 1];
+    if (threadIdx.x == 0) {
+        int t = 0;
+        seg_first[0] = 0;
+        for (int k = 0; k < kMaxSegs; ++k) {
+            if (k < G.n) t += *(volatile const int*)&(W.ctr + G.lane[k])->count[G.bounce[k]];
+            seg_first[k + 1] = t;
+        }
+    }
+    __syncthreads();
+    const int n = seg_first[kMaxSegs];
     const bool nee = nee_dl<NEE>(O) || nee_env<NEE>(O);
     const int lane = threadIdx.x & 31;
     const int stride = gridDim.x * blockDim.x;
     // uniform trip count across the warp so the append below runs converged
     for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
-        int slot = base + threadIdx.x;
+        const int item = base + threadIdx.x;
         bool alive = false;
-        int pid = 0;
-        if (slot < n) {
-            pid = ld_stream(&q[slot]);
-            int job_compact = compact;
+        int pid = 0, k = 0;
+        if (item < n) {
+            while (k + 1 < G.n && item >= seg_first[k + 1]) ++k;
+            const int slot = G.lane[k] * W.lane_stride + (item - seg_first[k]);
+            const int depth = G.bounce[k] + 1;
+            pid = ld_stream(&W.queue[G.bounce[k] & 1][slot]);
+            int job_compact = G.compact[k];
             const DevScene* sp = &S0;
             if (JOBS) {
                 const DevJob& J = W.jobs[W.path_job[pid]];
@@ -773,14 +789,19 @@ __global__ void __launch_bounds__(kShadeBlock, 16) k_shade(const __grid_constant
                 }
             }
         }
-        // warp-aggregated survivor append (src/kernels/shade_path.cu:355-363)
-        unsigned am = __ballot_sync(0xffffffffu, alive);
+        // warp-aggregated survivor append (src/kernels/shade_path.cu:355-363), one atomic per
+        // segment present in the warp
+        const unsigned am = __ballot_sync(0xffffffffu, alive);
         if (am) {
-            int b = 0;
-            int leader = __ffs(am) - 1;
-            if (lane == leader) b = atomicAdd(&W.ctr->count[depth], __popc(am));
-            b = __shfl_sync(0xffffffffu, b, leader);
-            if (alive) st_stream(&nq[b + __popc(am & ((1u << lane) - 1u))], pid);
+            const unsigned grp = __match_any_sync(0xffffffffu, alive ? k : -1);
+            if (alive) {
+                const int lk = G.lane[k], nb = G.bounce[k] + 1;
+                const int leader = __ffs(grp) - 1;
+                int b = 0;
+                if (lane == leader) b = atomicAdd(&(W.ctr + lk)->count[nb], __popc(grp));
+                b = __shfl_sync(grp, b, leader);
+                st_stream(&W.queue[nb & 1][lk * W.lane_stride + b + __popc(grp & ((1u << lane) - 1u))], pid);
+            }
         }
     }
 }
@@ -1061,26 +1082,33 @@ int shade_grid_blocks() {
 }
 
 cudaError_t launch_camera(const DevScene& S, const DevWave& W, const DevOptions& O, const DevCamera& C, int n,
-                          cudaStream_t st) {
+                          int lane, const int* wave_iter, cudaStream_t st) {
+    if (n > W.lane_stride || lane < 0) return cudaErrorInvalidValue;
     int grid = std::min((n + kShadeBlock - 1) / kShadeBlock, shade_grid_blocks() * 2);
     if (grid < 1) grid = 1;
-    k_camera<<<grid, kShadeBlock, 0, st>>>(S, W, O, C, n);
+    k_camera<<<grid, kShadeBlock, 0, st>>>(S, W, O, C, n, lane, wave_iter);
     return cudaGetLastError();
 }
 
 cudaError_t launch_shade(const DevScene& S, const DevWave& W, const DevOptions& O, int bounce, int compact,
                          cudaStream_t st) {
+    return launch_shade_segs(S, W, O, one_seg(bounce, compact), st);
+}
+
+cudaError_t launch_shade_segs(const DevScene& S, const DevWave& W, const DevOptions& O, const Segs& G,
+                              cudaStream_t st) {
+    if (G.n < 1 || G.n > kMaxSegs) return cudaErrorInvalidValue;
     const int g = shade_grid_blocks(), mode = nee_mode_of(O);
     if (O.material_debug && !W.path_job) {
-        k_shade<false, true, -1><<<g, kShadeBlock, 0, st>>>(S, W, O, bounce, compact);
+        k_shade<false, true, -1><<<g, kShadeBlock, 0, st>>>(S, W, O, G);
     } else if (W.path_job) {
-        if (mode == 2) k_shade<true, false, 2><<<g, kShadeBlock, 0, st>>>(S, W, O, bounce, compact);
-        else if (mode == 1) k_shade<true, false, 1><<<g, kShadeBlock, 0, st>>>(S, W, O, bounce, compact);
-        else k_shade<true, false, 0><<<g, kShadeBlock, 0, st>>>(S, W, O, bounce, compact);
+        if (mode == 2) k_shade<true, false, 2><<<g, kShadeBlock, 0, st>>>(S, W, O, G);
+        else if (mode == 1) k_shade<true, false, 1><<<g, kShadeBlock, 0, st>>>(S, W, O, G);
+        else k_shade<true, false, 0><<<g, kShadeBlock, 0, st>>>(S, W, O, G);
     } else {
-        if (mode == 2) k_shade<false, false, 2><<<g, kShadeBlock, 0, st>>>(S, W, O, bounce, compact);
-        else if (mode == 1) k_shade<false, false, 1><<<g, kShadeBlock, 0, st>>>(S, W, O, bounce, compact);
-        else k_shade<false, false, 0><<<g, kShadeBlock, 0, st>>>(S, W, O, bounce, compact);
+        if (mode == 2) k_shade<false, false, 2><<<g, kShadeBlock, 0, st>>>(S, W, O, G);
+        else if (mode == 1) k_shade<false, false, 1><<<g, kShadeBlock, 0, st>>>(S, W, O, G);
+        else k_shade<false, false, 0><<<g, kShadeBlock, 0, st>>>(S, W, O, G);
     }
     return cudaGetLastError();
 }
@@ -1097,11 +1125,12 @@ cudaError_t launch_accumulate_jobs(const DevWave& W, int compensated, cudaStream
     return cudaGetLastError();
 }
 
-cudaError_t launch_accumulate(const DevWave& W, float* image, float* comp, int nsamples, int compensated,
+cudaError_t launch_accumulate(const DevWave& W, int lane, float* image, float* comp, int nsamples, int compensated,
                               cudaStream_t st) {
+    if (lane < 0 || size_t(nsamples) * size_t(W.npix) > size_t(W.lane_stride)) return cudaErrorInvalidValue;
     int grid = std::min((W.npix + 255) / 256, 148 * 8);
     if (grid < 1) grid = 1;
-    k_accumulate<<<grid, 256, 0, st>>>(W.s3, image, comp, W.npix, nsamples, compensated);
+    k_accumulate<<<grid, 256, 0, st>>>(W.s3 + size_t(lane) * W.lane_stride, image, comp, W.npix, nsamples, compensated);
     return cudaGetLastError();
 }
 

@@ -407,7 +407,7 @@ struct Tracer {
 struct TraceArgs {
     DevScene S;
     DevWave W;
-    int bounce;
+    Segs G;      // the (lane, bounce) segments of the launch
     int mode;    // 0 radiance, 1 DL shadow, 2 env shadow, 3 BVH heatmap of radiance rays
     int nee;     // radiance pass: 0 none, 1 DL, 2 env
     const float* ext_rays;  // lux_trace_rays: rays given directly (n * 8 floats)
@@ -457,21 +457,38 @@ template <int MODE, bool SINGLE>
 // eight (64, with spills).
 __global__ void __launch_bounds__(kTraceBlock, 7) k_trace(const __grid_constant__ TraceArgs A) {
     __shared__ uint2 stack[kShStack][kTraceBlock];
-    Tracer<MODE, SINGLE> T{A.S, stack, {}, int(threadIdx.x), &A.W.ctr->error};
+    // work of segment k: items [seg_first[k], seg_first[k + 1]) of the launch's list
+    __shared__ int seg_first[kMaxSegs + 1];
+    const bool ext = A.ext_rays != nullptr;
+    if (threadIdx.x == 0) {
+        int t = 0;
+        seg_first[0] = 0;
+        for (int k = 0; k < kMaxSegs; ++k) {
+            if (!ext && k < A.G.n) {
+                const WaveCounters* c = A.W.ctr + A.G.lane[k];
+                t += (MODE == 0 || MODE == 3) ? *(volatile const int*)&c->count[A.G.bounce[k]]
+                                              : *(volatile const int*)&c->shadow[A.G.bounce[k]];
+            }
+            seg_first[k + 1] = t;
+        }
+    }
+    __syncthreads();
+    Tracer<MODE, SINGLE> T{A.S, stack, {}, int(threadIdx.x), &(A.W.ctr + A.G.lane[0])->error};
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    const bool ext = A.ext_rays != nullptr;
     int total;
     int* cursor;
+    // the cursor of the first segment's (lane, bounce) serves the whole launch: no other
+    // launch of this kind covers that lane at that bounce
     if (ext) {
         total = A.ext_n;
         cursor = A.ext_fetch;
     } else if (MODE == 0 || MODE == 3) {
-        total = *(volatile int*)&A.W.ctr->count[A.bounce];
-        cursor = &A.W.ctr->fetch_r[A.bounce];
+        total = seg_first[kMaxSegs];
+        cursor = &(A.W.ctr + A.G.lane[0])->fetch_r[A.G.bounce[0]];
     } else {
-        total = *(volatile int*)&A.W.ctr->shadow[A.bounce];
-        cursor = &A.W.ctr->fetch_s[A.bounce];
+        total = seg_first[kMaxSegs];
+        cursor = &(A.W.ctr + A.G.lane[0])->fetch_s[A.G.bounce[0]];
     }
     Lane L;
     bool active = false;
@@ -503,7 +520,10 @@ __global__ void __launch_bounds__(kTraceBlock, 7) k_trace(const __grid_constant_
                         L.pixel = __float_as_int(ry[7]);
                         L.iter = A.ext_iter;
                     } else if (MODE == 0 || MODE == 3) {
-                        int pid = ld_stream(&A.W.queue[A.bounce & 1][r]);
+                        int k = 0;
+                        while (k + 1 < A.G.n && r >= seg_first[k + 1]) ++k;
+                        item = A.G.lane[k] * A.W.lane_stride + (r - seg_first[k]);  // absolute slot
+                        int pid = ld_stream(&A.W.queue[A.G.bounce[k] & 1][item]);
                         float4 a = ld_stream(&A.W.s0[pid]), b = ld_stream(&A.W.s1[pid]);
                         o = mk(a.x, a.y, a.z);
                         d = mk(b.x, b.y, b.z);
@@ -512,13 +532,15 @@ __global__ void __launch_bounds__(kTraceBlock, 7) k_trace(const __grid_constant_
                         L.iter = __float_as_int(ld_stream(&A.W.s3[pid]).w);
                         if (A.W.path_job) root = A.W.jobs[A.W.path_job[pid]].tlas_root;
                     } else {
-                        int slot = ld_stream(&A.W.sh_queue[r]);
+                        int k = 0;
+                        while (k + 1 < A.G.n && r >= seg_first[k + 1]) ++k;
+                        int slot = ld_stream(&A.W.sh_queue[A.G.lane[k] * A.W.lane_stride + (r - seg_first[k])]);
                         item = slot;
                         float4 a = ld_stream(&A.W.sh_o[slot]), b = ld_stream(&A.W.sh_d[slot]);
                         o = mk(a.x, a.y, a.z);
                         d = mk(b.x, b.y, b.z);
                         tmax = a.w;
-                        int pid = ld_stream(&A.W.queue[A.bounce & 1][slot]);
+                        int pid = ld_stream(&A.W.queue[A.G.bounce[k] & 1][slot]);
                         L.pixel = __float_as_int(ld_stream(&A.W.s2[pid]).w);
                         L.iter = __float_as_int(ld_stream(&A.W.s3[pid]).w);
                         if (A.W.path_job) root = A.W.jobs[A.W.path_job[pid]].tlas_root;
@@ -589,7 +611,14 @@ __global__ void __launch_bounds__(kTraceBlock, 7) k_trace(const __grid_constant_
                                    __fadd_rn(wo.z, __fmul_rn(L.best.t, wd.z)));
                         f3 so = mk(__fadd_rn(hp.x, __fmul_rn(n.x, 1e-4f)), __fadd_rn(hp.y, __fmul_rn(n.y, 1e-4f)),
                                    __fadd_rn(hp.z, __fmul_rn(n.z, 1e-4f)));
-                        int pid = ld_stream(&A.W.queue[A.bounce & 1][item]);
+                        // the segment of this slot: its lane, then the segment holding that lane
+                        int k = 0;
+                        if (A.G.n > 1) {
+                            const int ln = item / A.W.lane_stride;
+                            while (k + 1 < A.G.n && A.G.lane[k] != ln) ++k;
+                        }
+                        const int bk = A.G.bounce[k], lk = A.G.lane[k];
+                        int pid = ld_stream(&A.W.queue[bk & 1][item]);
                         float4 ns = ld_stream(&A.W.s4[pid]);
                         f3 sd;
                         float tmax;
@@ -605,13 +634,14 @@ __global__ void __launch_bounds__(kTraceBlock, 7) k_trace(const __grid_constant_
                         }
                         st_stream(&A.W.sh_o[item], make_float4(so.x, so.y, so.z, tmax));
                         st_stream(&A.W.sh_d[item], make_float4(sd.x, sd.y, sd.z, 0.0f));
-                        // warp-aggregated append to the shadow queue
-                        unsigned am = __activemask();
+                        // append to the lane's shadow queue, aggregated over the lanes of the
+                        // warp that append to the same one
+                        const unsigned am = __match_any_sync(__activemask(), lk);
                         int leader = __ffs(am) - 1;
                         int b2 = 0;
-                        if (lane == leader) b2 = atomicAdd(&A.W.ctr->shadow[A.bounce], __popc(am));
+                        if (lane == leader) b2 = atomicAdd(&(A.W.ctr + lk)->shadow[bk], __popc(am));
                         b2 = __shfl_sync(am, b2, leader);
-                        st_stream(&A.W.sh_queue[b2 + __popc(am & ((1u << lane) - 1u))], item);
+                        st_stream(&A.W.sh_queue[lk * A.W.lane_stride + b2 + __popc(am & ((1u << lane) - 1u))], item);
                     }
                 } else if (MODE == 1) {
                     bool hit = L.best.inst >= 0;
@@ -619,7 +649,7 @@ __global__ void __launch_bounds__(kTraceBlock, 7) k_trace(const __grid_constant_
                     st_stream(&A.W.sh_prim[item], L.best.prim);
                 } else if (MODE == 3) {
                     // drawBVH (src/kernels/draw_bvh.cu:33): color += count * 0.001 on every channel
-                    int pid = A.W.queue[A.bounce & 1][item];
+                    int pid = A.W.queue[A.G.bounce[0] & 1][item];  // the heatmap traces one wave
                     float4 c = A.W.s3[pid];
                     const float h = float(L.work) * 0.001f;
                     A.W.s3[pid] = make_float4(c.x + h, c.y + h, c.z + h, c.w);
@@ -677,7 +707,13 @@ void launch_mode(int mode, int grid, cudaStream_t st, const TraceArgs& A) {
 
 cudaError_t launch_trace(const DevScene& S, const DevWave& W, int bounce, int mode, int nee, cudaStream_t st,
                          int grid) {
-    TraceArgs A{S, W, bounce, mode, nee, nullptr, nullptr, 0, 0, nullptr};
+    return launch_trace_segs(S, W, one_seg(bounce), mode, nee, st, grid);
+}
+
+cudaError_t launch_trace_segs(const DevScene& S, const DevWave& W, const Segs& G, int mode, int nee, cudaStream_t st,
+                              int grid) {
+    if (G.n < 1 || G.n > kMaxSegs) return cudaErrorInvalidValue;
+    TraceArgs A{S, W, G, mode, nee, nullptr, nullptr, 0, 0, nullptr};
     const bool single = S.single_level != 0;
     if (grid <= 0) grid = trace_grid_blocks(mode, single);
     if (single) launch_mode<true>(mode, grid, st, A);
@@ -687,7 +723,7 @@ cudaError_t launch_trace(const DevScene& S, const DevWave& W, int bounce, int mo
 
 cudaError_t launch_trace_ext(const DevScene& S, const DevWave& W, const float* rays, uint32_t* hits, int n, int mode,
                              int iter, int* fetch, cudaStream_t st) {
-    TraceArgs A{S, W, 0, mode, 0, rays, hits, n, iter, fetch};
+    TraceArgs A{S, W, one_seg(0), mode, 0, rays, hits, n, iter, fetch};
     const bool single = S.single_level != 0;
     const int grid = trace_grid_blocks(mode, single);
     if (single) launch_mode<true>(mode, grid, st, A);

@@ -294,6 +294,43 @@ def test_batched_waves_graphs_and_sorting_give_identical_images():
         assert np.array_equal(bits(im), bits(imgs[0]))
 
 
+@pytest.mark.parametrize("depth", [2, 5, 8])
+def test_pipelined_waves_give_identical_images(depth):
+    """Several waves in flight (one per lane, each bounce step launched over all of them) give
+    the image of one wave at a time bit for bit: with graphs and without, timed, split over two
+    calls, and for trace depths that give 2, 4 and 4 lanes. The counters of the last wave are
+    those of that wave rendered alone."""
+    s = small_random_scene(seed=12, width=40, height=32)
+    base = dict(direct_light_sampling=1, env_importance_sampling=1, trace_depth=depth)
+    r = lx.Renderer(s, default_options(**base))
+    for it in range(1, 8):
+        r.render_iter(it)
+    ref = bits(r.image_sum())
+    p_ref, s_ref = r.wave_counts(depth + 1)
+    r.close()
+    for kw in (dict(spp_per_wave=1), dict(spp_per_wave=2), dict(spp_per_wave=3, use_graph=0)):
+        r = lx.Renderer(s, default_options(**base, **kw))
+        r.render(1, 7)
+        assert np.array_equal(bits(r.image_sum()), ref), kw
+        st = r.stats()
+        assert st["samples"] == 7 * 40 * 32
+        if kw["spp_per_wave"] == 1:
+            p, sh = r.wave_counts(depth + 1)
+            assert np.array_equal(p, p_ref) and np.array_equal(sh, s_ref)
+        r.reset()
+        r.render(1, 3)
+        r.render(4, 4)
+        assert np.array_equal(bits(r.image_sum()), ref), ("two calls", kw)
+        r.reset()
+        r.enable_timing(True)
+        r.render(1, 7)
+        r.enable_timing(False)
+        st = r.stats()
+        assert np.array_equal(bits(r.image_sum()), ref), ("timed", kw)
+        assert st["ms_trace"] > 0 and st["ms_shade"] > 0 and st["ms_camera"] > 0
+        r.close()
+
+
 def test_white_furnace():
     """A smooth white metal sphere (F = 1, G ~ 1) under a constant environment of 1: every
     pixel converges to 1 (energy conservation within 1e-3)."""
