@@ -428,7 +428,7 @@ typedef struct lux_engine_stats {
     int64_t waves;
     double samples;           /* pixel samples rendered                                         */
     double rays;              /* radiance + shadow rays traced                                  */
-    double ms_device;         /* summed wave times (CUDA events)                                */
+    double ms_device;         /* summed device time of the steps (CUDA events)                  */
     int64_t device_bytes;     /* scenes + wave buffers + live job images                        */
     int64_t scene_bytes;
     int32_t max_paths;        /* wave size in use (autotuned when configured 0)                 */
@@ -440,8 +440,11 @@ int lux_engine_create(const lux_scene_desc* const* scenes, int num_scenes, const
                       const lux_engine_config* cfg, lux_engine** out);
 /* Queue a job; *job_id identifies it from then on. */
 int lux_engine_submit(lux_engine* e, const lux_job_desc* job, int* job_id);
-/* Admit what fits, render one wave, and return how many jobs completed in it (*done_jobs may
- * be NULL). *idle is set to 1 when there was nothing to render. */
+/* Admit what fits and advance the shared wavefront; return how many jobs completed (*done_jobs
+ * may be NULL). The first waves (the autotuning ones) run one whole wave per call; after them
+ * up to four waves are in flight: a call starts a new wave when a lane is free and there is
+ * work, advances every wave in flight by three bounces, and accumulates the waves that are
+ * through, in the order they started. *idle is set to 1 when there was nothing to render. */
 int lux_engine_step(lux_engine* e, int* done_jobs, int* idle);
 /* Step until every submitted job is done. */
 int lux_engine_run(lux_engine* e);

@@ -136,11 +136,13 @@ struct lux_ctx {
     // pipelined call; both hold device and page-locked host pointers of this context
     std::map<int, cudaGraphExec_t> graphs;
     std::map<std::pair<int, int>, cudaGraphExec_t> pgraphs;  // (waves, last wave size)
+    std::map<std::pair<int, int>, int> pseen;                // call shapes launched eagerly
     void drop_graphs() {
         for (auto& g : graphs) cudaGraphExecDestroy(g.second);
         graphs.clear();
         for (auto& g : pgraphs) cudaGraphExecDestroy(g.second);
         pgraphs.clear();
+        pseen.clear();
     }
     // stats of the last call
     lux_stats stats{};
@@ -929,9 +931,12 @@ int run_pipelined(lux_ctx* C, int first_iter, int n_iter, int nwaves, int lanes)
         }
         LUX_CUDA(cudaMemcpyAsync(C->W.wave_iter, &C->h_wave_iter[2 * c0], 2 * sizeof(int) * size_t(nw),
                                  cudaMemcpyHostToDevice, st));
-        if (C->opt.use_graph && !C->timing) {
-            // the graph bakes in the chunk's counter copies (h_ctr + c0) and its wave count
-            const std::pair<int, int> key{(c0 / kWaveTab) * (kWaveTab + 1) + nw, ns_last};
+        // the graph bakes in the chunk's counter copies (h_ctr + c0) and its wave count. A call
+        // shape is captured when it comes again: a context that renders once (a cold start,
+        // a one-off job) would spend more on capturing and instantiating than replay saves.
+        const std::pair<int, int> key{(c0 / kWaveTab) * (kWaveTab + 1) + nw, ns_last};
+        const bool replay = C->opt.use_graph && !C->timing && (C->pgraphs.count(key) || C->pseen[key]++ > 0);
+        if (replay) {
             auto it = C->pgraphs.find(key);
             if (it == C->pgraphs.end()) {
                 cudaGraph_t g;

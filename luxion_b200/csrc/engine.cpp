@@ -45,6 +45,19 @@ struct EngineJob {
     double t_submit = 0, t_admit = 0, t_done = 0;
 };
 
+// A wave in flight (after autotuning, up to kEngineLanes at once): its lane, the depth it runs
+// to, the next bounce, its paths and the (job id, samples) it renders.
+struct Flight {
+    int lane = 0;
+    int depth = 0;
+    int bounce = 0;
+    int paths = 0;
+    std::vector<std::pair<int, int>> part;
+};
+constexpr int kEngineLanes = kMaxSegs;
+// bounces every wave in flight advances per lux_engine_step
+constexpr int kStepBounces = 3;
+
 double now_ms(std::chrono::steady_clock::time_point t0) {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -72,10 +85,12 @@ struct lux_engine {
     int trace_blocks = 0;         // persistent trace grid in use
     DevJob* jobs_d = nullptr;
     DevJob* jobs_h = nullptr;     // pinned mirror, one row per slot
-    DevSegment* segs_d = nullptr;
-    DevSegment* segs_h = nullptr; // pinned
-    int* hdr_h = nullptr;         // pinned, 4 ints
-    WaveCounters* ctr_h = nullptr;
+    DevSegment* segs_d = nullptr; // per lane, kMaxSegments each
+    DevSegment* segs_h = nullptr; // pinned, per lane
+    int* hdr_h = nullptr;         // pinned, 4 ints per lane
+    WaveCounters* ctr_h = nullptr;  // pinned, per lane
+    int lanes = kEngineLanes;
+    std::deque<Flight> flight;    // waves in flight, in start order
     int max_jobs = 0;
     std::vector<int> free_slots;
     std::vector<EngineJob> jobs;  // by job id
@@ -139,13 +154,13 @@ int enqueue_wave(lux_engine* E, int depth, int wave_paths, int trace_grid) {
     cudaStream_t st = E->stream;
     const int nee = E->dopt.env ? 2 : (E->dopt.dl ? 1 : 0);
     LUX_CUDA(cudaMemsetAsync(E->W.ctr, 0, sizeof(WaveCounters), st));
-    LUX_CUDA(launch_camera_jobs(E->W, E->dopt, wave_paths, st));
+    LUX_CUDA(launch_camera_jobs(E->W, E->dopt, wave_paths, 0, st));
     for (int b = 0; b < depth; ++b) {
         LUX_CUDA(launch_trace(E->S, E->W, b, 0, nee, st, trace_grid));
         if (nee) LUX_CUDA(launch_trace(E->S, E->W, b, nee == 2 ? 2 : 1, 0, st, trace_grid));
         LUX_CUDA(launch_shade(E->S, E->W, E->dopt, b, 1, st));
     }
-    LUX_CUDA(launch_accumulate_jobs(E->W, E->opt.precision == LUX_PRECISION_COMPENSATED, st));
+    LUX_CUDA(launch_accumulate_jobs(E->W, E->opt.precision == LUX_PRECISION_COMPENSATED, 0, st));
     return LUX_OK;
 }
 
@@ -323,15 +338,16 @@ int lux_engine_create(const lux_scene_desc* const* scenes, int num_scenes, const
     static const int kTuneSizes[] = {2 << 20, 4 << 20, 8 << 20};
     E->paths_alloc = c.max_paths > 0 ? c.max_paths : kTuneSizes[2];
     DevWave& W = E->W;
-    const size_t n = size_t(E->paths_alloc);
+    const int L = E->lanes;
+    const size_t n = size_t(E->paths_alloc) * size_t(L);  // lane l: paths [l * paths_alloc, ...)
     int rc;
     if ((rc = E->alloc(&W.s0, n)) || (rc = E->alloc(&W.s1, n)) || (rc = E->alloc(&W.s2, n)) ||
         (rc = E->alloc(&W.s3, n)) || (rc = E->alloc(&W.s4, n)) || (rc = E->alloc(&W.queue[0], n)) ||
         (rc = E->alloc(&W.queue[1], n)) || (rc = E->alloc(&W.hit, n)) || (rc = E->alloc(&W.hit_prim, n)) ||
         (rc = E->alloc(&W.sh_o, n)) || (rc = E->alloc(&W.sh_d, n)) || (rc = E->alloc(&W.sh_queue, n)) ||
-        (rc = E->alloc(&W.sh_hit, n)) || (rc = E->alloc(&W.sh_prim, n)) || (rc = E->alloc(&W.ctr, 1)) ||
+        (rc = E->alloc(&W.sh_hit, n)) || (rc = E->alloc(&W.sh_prim, n)) || (rc = E->alloc(&W.ctr, size_t(L))) ||
         (rc = E->alloc(&W.wave_iter, 4)) || (rc = E->alloc(&W.path_job, n)) ||
-        (rc = E->alloc(&E->segs_d, kMaxSegments)) || (rc = E->alloc(&W.wave_hdr, 4)))
+        (rc = E->alloc(&E->segs_d, size_t(kMaxSegments) * L)) || (rc = E->alloc(&W.wave_hdr, size_t(4) * L)))
         return bail(rc);
     E->max_jobs = c.max_jobs > 0 ? c.max_jobs : 4096;
     if ((rc = E->alloc(&E->jobs_d, size_t(E->max_jobs)))) return bail(rc);
@@ -339,11 +355,11 @@ int lux_engine_create(const lux_scene_desc* const* scenes, int num_scenes, const
     W.jobs = E->jobs_d;
     W.segs = E->segs_d;
     W.max_paths = E->paths_alloc;
-    W.lane_stride = E->paths_alloc;  // one lane
+    W.lane_stride = E->paths_alloc;
     if (cudaMallocHost(&E->jobs_h, sizeof(DevJob) * E->max_jobs) != cudaSuccess ||
-        cudaMallocHost(&E->segs_h, sizeof(DevSegment) * kMaxSegments) != cudaSuccess ||
-        cudaMallocHost(&E->hdr_h, sizeof(int) * 4) != cudaSuccess ||
-        cudaMallocHost(&E->ctr_h, sizeof(WaveCounters)) != cudaSuccess)
+        cudaMallocHost(&E->segs_h, sizeof(DevSegment) * kMaxSegments * L) != cudaSuccess ||
+        cudaMallocHost(&E->hdr_h, sizeof(int) * 4 * L) != cudaSuccess ||
+        cudaMallocHost(&E->ctr_h, sizeof(WaveCounters) * L) != cudaSuccess)
         return bail(fail(LUX_ERR_OOM, "pinned host allocation failed"));
     for (int s = E->max_jobs - 1; s >= 0; --s) E->free_slots.push_back(s);
     cudaEventCreate(&E->ev[0]);
@@ -394,18 +410,22 @@ int lux_engine_submit(lux_engine* E, const lux_job_desc* job, int* job_id) {
     return LUX_OK;
 }
 
-int lux_engine_step(lux_engine* E, int* done_jobs, int* idle) {
-    if (!E) return fail(LUX_ERR_INVALID, "engine is NULL");
-    if (done_jobs) *done_jobs = 0;
-    if (idle) *idle = 0;
-    LUX_CUDA(cudaSetDevice(E->device));
-    if (int rc = admit(E)) return rc;
-    // autotuning: the first waves try each candidate once; then the cheapest per path stays
-    const bool tuning = E->tune_next < E->tune_cands.size();
-    if (tuning) {
-        E->max_paths = E->tune_cands[E->tune_next].first;
-        E->trace_blocks = E->tune_cands[E->tune_next].second;
-    }
+}  // extern "C"
+
+namespace {
+
+// The wave's view of the engine's arrays in lane `lane`: its own segment table and header.
+DevWave lane_view(const lux_engine* E, int lane) {
+    DevWave W = E->W;
+    W.segs = E->segs_d + size_t(lane) * kMaxSegments;
+    W.wave_hdr = E->W.wave_hdr + size_t(lane) * 4;
+    return W;
+}
+
+// Plan the next wave into lane `lane`'s host tables and copy them to the device: returns its
+// segments (0: nothing to render) with its size, depth, paths and (job id, samples) parts.
+int plan_next(lux_engine* E, int lane, int& wave_paths, int& depth, int& path0,
+              std::vector<std::pair<int, int>>& part) {
     std::vector<int> order;
     const int nj = order_jobs(E, order);
     std::vector<int> np(nj), rem(nj), take(nj);
@@ -414,7 +434,7 @@ int lux_engine_step(lux_engine* E, int* done_jobs, int* idle) {
         np[i] = j.npix;
         rem[i] = j.desc.spp - j.spp_sched;
     }
-    int wave_paths = E->max_paths;
+    wave_paths = E->max_paths;
     int nsegs = lux_plan_wave(np.data(), rem.data(), nj, wave_paths, kMaxSegments, take.data());
     if (nsegs <= 0 && nj > 0) {
         // one sample of every waiting job exceeds the wave size in use (a small autotuning
@@ -422,16 +442,17 @@ int lux_engine_step(lux_engine* E, int* done_jobs, int* idle) {
         wave_paths = E->paths_alloc;
         nsegs = lux_plan_wave(np.data(), rem.data(), nj, wave_paths, kMaxSegments, take.data());
     }
-    if (nsegs <= 0) {
-        if (idle) *idle = 1;
-        return LUX_OK;
-    }
-    int path0 = 0, pix0 = 0, k = 0, depth = 0;
-    std::vector<std::pair<int, int>> part;  // (job id, samples)
+    if (nsegs <= 0) return 0;
+    DevSegment* segs_h = E->segs_h + size_t(lane) * kMaxSegments;
+    int* hdr_h = E->hdr_h + size_t(lane) * 4;
+    path0 = 0;
+    depth = 0;
+    part.clear();
+    int pix0 = 0, k = 0;
     for (int i = 0; i < nj; ++i) {
         if (!take[i]) continue;
         EngineJob& j = E->jobs[order[i]];
-        E->segs_h[k] = DevSegment{j.slot, j.spp_sched, take[i], path0, pix0};
+        segs_h[k] = DevSegment{j.slot, j.spp_sched, take[i], path0, pix0};
         path0 += take[i] * j.npix;
         pix0 += j.npix;
         depth = std::max(depth, j.depth);
@@ -439,12 +460,57 @@ int lux_engine_step(lux_engine* E, int* done_jobs, int* idle) {
         part.push_back({order[i], take[i]});
         ++k;
     }
-    E->hdr_h[0] = k;
-    E->hdr_h[1] = path0;
-    E->hdr_h[2] = pix0;
+    hdr_h[0] = k;
+    hdr_h[1] = path0;
+    hdr_h[2] = pix0;
     cudaStream_t st = E->stream;
-    LUX_CUDA(cudaMemcpyAsync(E->segs_d, E->segs_h, sizeof(DevSegment) * k, cudaMemcpyHostToDevice, st));
-    LUX_CUDA(cudaMemcpyAsync(E->W.wave_hdr, E->hdr_h, sizeof(int) * 4, cudaMemcpyHostToDevice, st));
+    LUX_CUDA(cudaMemcpyAsync(E->segs_d + size_t(lane) * kMaxSegments, segs_h, sizeof(DevSegment) * k,
+                             cudaMemcpyHostToDevice, st));
+    LUX_CUDA(cudaMemcpyAsync(E->W.wave_hdr + size_t(lane) * 4, hdr_h, sizeof(int) * 4, cudaMemcpyHostToDevice, st));
+    return k;
+}
+
+// Bookkeeping of a wave that has been accumulated (its counters copied to c): rays, samples,
+// and the jobs it completed.
+int finish_wave(lux_engine* E, const WaveCounters& c, int depth, int paths, const std::vector<std::pair<int, int>>& part) {
+    if (c.error) return fail(LUX_ERR_UNSUPPORTED, "traversal stack overflow");
+    const double t = now_ms(E->t0);
+    double rays = 0;
+    for (int b = 0; b < depth; ++b) rays += double(c.count[b]) + double(c.shadow[b]);
+    E->stats.waves += 1;
+    E->stats.samples += double(paths);
+    E->stats.rays += rays;
+    int done = 0;
+    for (auto& pr : part) {
+        EngineJob& j = E->jobs[pr.first];
+        j.spp_done += pr.second;
+        j.waves += 1;
+        if (j.spp_done == j.desc.spp) {
+            j.state = LUX_JOB_DONE;
+            j.t_done = t;
+            ++done;
+        }
+    }
+    if (done) {
+        std::vector<int> keep;
+        for (int id : E->active)
+            if (E->jobs[id].state == LUX_JOB_ACTIVE) keep.push_back(id);
+        E->active.swap(keep);
+    }
+    return done;
+}
+
+// One wave start to end, as a CUDA graph (the autotuning waves).
+int step_one_wave(lux_engine* E, bool tuning, int* done_jobs, int* idle) {
+    int wave_paths = 0, depth = 0, path0 = 0;
+    std::vector<std::pair<int, int>> part;
+    const int k = plan_next(E, 0, wave_paths, depth, path0, part);
+    if (k < 0) return k;
+    if (k == 0) {
+        if (idle) *idle = 1;
+        return LUX_OK;
+    }
+    cudaStream_t st = E->stream;
     auto key = std::make_tuple(depth, wave_paths, E->trace_blocks);
     auto it = E->graphs.find(key);
     if (it == E->graphs.end()) {
@@ -465,15 +531,8 @@ int lux_engine_step(lux_engine* E, int* done_jobs, int* idle) {
     LUX_CUDA(cudaEventRecord(E->ev[1], st));
     LUX_CUDA(cudaMemcpyAsync(E->ctr_h, E->W.ctr, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st));
     LUX_CUDA(cudaStreamSynchronize(st));
-    if (E->ctr_h->error) return fail(LUX_ERR_UNSUPPORTED, "traversal stack overflow");
     float ms = 0;
     cudaEventElapsedTime(&ms, E->ev[0], E->ev[1]);
-    const double t = now_ms(E->t0);
-    double rays = 0;
-    for (int b = 0; b < depth; ++b) rays += double(E->ctr_h->count[b]) + double(E->ctr_h->shadow[b]);
-    E->stats.waves += 1;
-    E->stats.samples += double(path0);
-    E->stats.rays += rays;
     E->stats.ms_device += ms;
     if (tuning) {
         E->tune_cost.push_back(double(ms) / std::max(1, path0));
@@ -483,25 +542,101 @@ int lux_engine_step(lux_engine* E, int* done_jobs, int* idle) {
             E->trace_blocks = E->tune_cands[best].second;
         }
     }
-    int done = 0;
-    for (auto& pr : part) {
-        EngineJob& j = E->jobs[pr.first];
-        j.spp_done += pr.second;
-        j.waves += 1;
-        if (j.spp_done == j.desc.spp) {
-            j.state = LUX_JOB_DONE;
-            j.t_done = t;
-            ++done;
+    const int done = finish_wave(E, *E->ctr_h, depth, path0, part);
+    if (done < 0) return done;
+    if (done_jobs) *done_jobs = done;
+    return LUX_OK;
+}
+
+// Waves in flight (after autotuning): start a wave in a free lane when there is work, advance
+// every wave in flight by kStepBounces bounces in launches that cover all of them, then
+// accumulate the waves that are through, in start order, so each job's samples add up in
+// sample order as in step_one_wave. A wave that ends before an older one keeps its lane until
+// the older one is done.
+int step_pipelined(lux_engine* E, int* done_jobs, int* idle) {
+    cudaStream_t st = E->stream;
+    const int nee = E->dopt.env ? 2 : (E->dopt.dl ? 1 : 0);
+    if (int(E->flight.size()) < E->lanes) {
+        int lane = 0;
+        for (; lane < E->lanes; ++lane) {
+            bool used = false;
+            for (const Flight& f : E->flight) used = used || f.lane == lane;
+            if (!used) break;
+        }
+        Flight f;
+        int wave_paths = 0;
+        const int k = plan_next(E, lane, wave_paths, f.depth, f.paths, f.part);
+        if (k < 0) return k;
+        if (k > 0) {
+            f.lane = lane;
+            LUX_CUDA(cudaMemsetAsync(E->W.ctr + lane, 0, sizeof(WaveCounters), st));
+            LUX_CUDA(launch_camera_jobs(lane_view(E, lane), E->dopt, wave_paths, lane, st));
+            E->flight.push_back(std::move(f));
         }
     }
-    if (done) {
-        std::vector<int> keep;
-        for (int id : E->active)
-            if (E->jobs[id].state == LUX_JOB_ACTIVE) keep.push_back(id);
-        E->active.swap(keep);
+    if (E->flight.empty()) {
+        if (idle) *idle = 1;
+        return LUX_OK;
+    }
+    LUX_CUDA(cudaEventRecord(E->ev[0], st));
+    for (int s = 0; s < kStepBounces; ++s) {
+        Segs G{};
+        for (const Flight& f : E->flight) {
+            if (f.bounce >= f.depth) continue;
+            G.lane[G.n] = f.lane;
+            G.bounce[G.n] = f.bounce;
+            G.compact[G.n] = 1;  // each path stops at its own job's depth
+            ++G.n;
+        }
+        if (G.n == 0) break;
+        LUX_CUDA(launch_trace_segs(E->S, E->W, G, 0, nee, st, E->trace_blocks));
+        if (nee) LUX_CUDA(launch_trace_segs(E->S, E->W, G, nee == 2 ? 2 : 1, 0, st, E->trace_blocks));
+        LUX_CUDA(launch_shade_segs(E->S, E->W, E->dopt, G, st));
+        for (Flight& f : E->flight)
+            if (f.bounce < f.depth) ++f.bounce;
+    }
+    std::vector<Flight> fin;
+    while (!E->flight.empty() && E->flight.front().bounce >= E->flight.front().depth) {
+        Flight f = std::move(E->flight.front());
+        E->flight.pop_front();
+        LUX_CUDA(launch_accumulate_jobs(lane_view(E, f.lane), E->opt.precision == LUX_PRECISION_COMPENSATED, f.lane, st));
+        LUX_CUDA(cudaMemcpyAsync(E->ctr_h + f.lane, E->W.ctr + f.lane, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st));
+        fin.push_back(std::move(f));
+    }
+    LUX_CUDA(cudaEventRecord(E->ev[1], st));
+    LUX_CUDA(cudaStreamSynchronize(st));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, E->ev[0], E->ev[1]);
+    E->stats.ms_device += ms;
+    int done = 0;
+    for (const Flight& f : fin) {
+        const int d = finish_wave(E, E->ctr_h[f.lane], f.depth, f.paths, f.part);
+        if (d < 0) return d;
+        done += d;
     }
     if (done_jobs) *done_jobs = done;
     return LUX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lux_engine_step(lux_engine* E, int* done_jobs, int* idle) {
+    if (!E) return fail(LUX_ERR_INVALID, "engine is NULL");
+    if (done_jobs) *done_jobs = 0;
+    if (idle) *idle = 0;
+    LUX_CUDA(cudaSetDevice(E->device));
+    if (int rc = admit(E)) return rc;
+    // autotuning: the first waves try each candidate once, one wave at a time; then the
+    // cheapest per path stays and waves run in flight together
+    const bool tuning = E->tune_next < E->tune_cands.size();
+    if (tuning) {
+        E->max_paths = E->tune_cands[E->tune_next].first;
+        E->trace_blocks = E->tune_cands[E->tune_next].second;
+        return step_one_wave(E, true, done_jobs, idle);
+    }
+    return step_pipelined(E, done_jobs, idle);
 }
 
 int lux_engine_run(lux_engine* E) {

@@ -45,10 +45,10 @@ cudaError_t launch_shade(const DevScene& S, const DevWave& W, const DevOptions& 
 // the same over several (lane, bounce) segments of waves in flight, in one launch
 cudaError_t launch_shade_segs(const DevScene& S, const DevWave& W, const DevOptions& O, const Segs& G,
                               cudaStream_t st);
-// job engine: camera rays of the wave's segments (counts read from W.wave_hdr), and the
-// per-job accumulation of the segments in sample order
-cudaError_t launch_camera_jobs(const DevWave& W, const DevOptions& O, int max_paths, cudaStream_t st);
-cudaError_t launch_accumulate_jobs(const DevWave& W, int compensated, cudaStream_t st);
+// job engine: camera rays of the wave's segments (W.segs, counts read from W.wave_hdr) into lane
+// `lane`, and the per-job accumulation of that lane's segments in sample order
+cudaError_t launch_camera_jobs(const DevWave& W, const DevOptions& O, int max_paths, int lane, cudaStream_t st);
+cudaError_t launch_accumulate_jobs(const DevWave& W, int compensated, int lane, cudaStream_t st);
 // image[p] (+comp) += radiance of every sample of the wave in lane `lane`, in sample order
 cudaError_t launch_accumulate(const DevWave& W, int lane, float* image, float* comp, int nsamples, int compensated,
                               cudaStream_t st);

@@ -859,16 +859,19 @@ LUX_DI int find_segment(const DevSegment* segs, int nsegs, int v) {
 // Camera rays of a job-engine wave (generateRayFromCamera, src/kernels/generate_ray_from_camera.cu:8-39,
 // per job): path pid belongs to the segment covering it; its sample s and pixel index give the
 // job-local iteration and pixel that seed the RNG, exactly as a single-job render would.
-__global__ void __launch_bounds__(kShadeBlock) k_camera_jobs(DevWave W, DevOptions O) {
+// W.segs and W.wave_hdr are the wave's own tables; its paths go to lane `lane`.
+__global__ void __launch_bounds__(kShadeBlock) k_camera_jobs(DevWave W, DevOptions O, int lane) {
     __shared__ DevSegment segs[kMaxSegments];
-    const int nsegs = W.wave_hdr[0], n = W.wave_hdr[1];
+    const int nsegs = W.wave_hdr[0], n = min(W.wave_hdr[1], W.lane_stride);
     for (int k = threadIdx.x; k < nsegs; k += blockDim.x) segs[k] = W.segs[k];
     __syncthreads();
     const bool nee = O.dl || O.env;
-    for (int pid = blockIdx.x * blockDim.x + threadIdx.x; pid < n; pid += gridDim.x * blockDim.x) {
-        const DevSegment& g = segs[find_segment<0>(segs, nsegs, pid)];
+    const int base = lane * W.lane_stride;
+    for (int local = blockIdx.x * blockDim.x + threadIdx.x; local < n; local += gridDim.x * blockDim.x) {
+        const int pid = base + local;
+        const DevSegment& g = segs[find_segment<0>(segs, nsegs, local)];
         const DevJob& J = W.jobs[g.job];
-        int off = pid - g.path0;
+        int off = local - g.path0;
         int s = off / J.npix, index = off - s * J.npix;
         int iter = J.first_iter + g.sample0 + s;
         int x = index % J.width, y = index / J.width;
@@ -892,14 +895,15 @@ __global__ void __launch_bounds__(kShadeBlock) k_camera_jobs(DevWave W, DevOptio
         W.path_job[pid] = g.job;
         W.queue[0][pid] = pid;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) W.ctr->count[0] = n;
+    if (blockIdx.x == 0 && threadIdx.x == 0) (W.ctr + lane)->count[0] = n;
 }
 
 // image[job pixel] (+comp) += radiance of the segment's samples, in sample order, so that a
 // job's image is the same bit for bit however its samples were split into waves.
-__global__ void k_accumulate_jobs(DevWave W, int compensated) {
+__global__ void k_accumulate_jobs(DevWave W, int compensated, int lane) {
     __shared__ DevSegment segs[kMaxSegments];
     const int nsegs = W.wave_hdr[0], total = W.wave_hdr[2];
+    const float4* __restrict__ s3 = W.s3 + size_t(lane) * W.lane_stride;
     for (int k = threadIdx.x; k < nsegs; k += blockDim.x) segs[k] = W.segs[k];
     __syncthreads();
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += gridDim.x * blockDim.x) {
@@ -913,7 +917,7 @@ __global__ void k_accumulate_jobs(DevWave W, int compensated) {
         if (compensated) {
             float cr = comp[o], cg = comp[o + 1], cb = comp[o + 2];
             for (int s = 0; s < g.nsamples; ++s) {
-                float4 c = W.s3[size_t(g.path0) + size_t(s) * J.npix + p];
+                float4 c = ld_stream(&s3[size_t(g.path0) + size_t(s) * J.npix + p]);
                 float yr = c.x - cr, tr = r + yr;
                 cr = (tr - r) - yr;
                 r = tr;
@@ -929,7 +933,7 @@ __global__ void k_accumulate_jobs(DevWave W, int compensated) {
             comp[o + 2] = cb;
         } else {
             for (int s = 0; s < g.nsamples; ++s) {
-                float4 c = W.s3[size_t(g.path0) + size_t(s) * J.npix + p];
+                float4 c = ld_stream(&s3[size_t(g.path0) + size_t(s) * J.npix + p]);
                 r += c.x;
                 gr += c.y;
                 b += c.z;
@@ -1113,15 +1117,17 @@ cudaError_t launch_shade_segs(const DevScene& S, const DevWave& W, const DevOpti
     return cudaGetLastError();
 }
 
-cudaError_t launch_camera_jobs(const DevWave& W, const DevOptions& O, int max_paths, cudaStream_t st) {
+cudaError_t launch_camera_jobs(const DevWave& W, const DevOptions& O, int max_paths, int lane, cudaStream_t st) {
+    if (lane < 0) return cudaErrorInvalidValue;
     int grid = std::min((max_paths + kShadeBlock - 1) / kShadeBlock, shade_grid_blocks() * 2);
     if (grid < 1) grid = 1;
-    k_camera_jobs<<<grid, kShadeBlock, 0, st>>>(W, O);
+    k_camera_jobs<<<grid, kShadeBlock, 0, st>>>(W, O, lane);
     return cudaGetLastError();
 }
 
-cudaError_t launch_accumulate_jobs(const DevWave& W, int compensated, cudaStream_t st) {
-    k_accumulate_jobs<<<148 * 8, 256, 0, st>>>(W, compensated);
+cudaError_t launch_accumulate_jobs(const DevWave& W, int compensated, int lane, cudaStream_t st) {
+    if (lane < 0) return cudaErrorInvalidValue;
+    k_accumulate_jobs<<<148 * 8, 256, 0, st>>>(W, compensated, lane);
     return cudaGetLastError();
 }
 

@@ -89,7 +89,12 @@ def test_budget_queues_jobs_and_progressive_results(scenes):
     E = lx.Engine([scenes["a"]], default_options(**OPT), max_paths=2000, hbm_budget_bytes=base + one_image + 16)
     cam = scenes["a"].desc.camera
     j1, j2 = E.submit(0, 3, camera=cam), E.submit(0, 2, camera=cam, first_iter=4)
-    E.step()
+    # a step advances the waves in flight by a few bounces; step until the first one is in
+    steps = 0
+    while E.status(j1)["spp_done"] == 0:
+        E.step()
+        steps += 1
+        assert steps < 64
     s1, s2 = E.status(j1), E.status(j2)
     assert s1["state"] == _ffi.JOB_ACTIVE and s1["spp_done"] == 1 and s2["state"] == _ffi.JOB_QUEUED
     assert same(E.image(j1), plain(scenes["a"], 1))          # progressive: 1 of 3 samples

@@ -317,6 +317,10 @@ def test_pipelined_waves_give_identical_images(depth):
         if kw["spp_per_wave"] == 1:
             p, sh = r.wave_counts(depth + 1)
             assert np.array_equal(p, p_ref) and np.array_equal(sh, s_ref)
+        for rep in range(2):  # the call shape again: captured as a graph, then replayed
+            r.reset()
+            r.render(1, 7)
+            assert np.array_equal(bits(r.image_sum()), ref), ("again", rep, kw)
         r.reset()
         r.render(1, 3)
         r.render(4, 4)
