@@ -564,11 +564,16 @@ def main():
     ach = trace_bytes_per_launch / (trace_ms_per_launch * 1e-3) / 1e9
     shade_bytes = SHADE_BYTES_PER_BOUNCE * kt["path_bounces"]
     shade_ach = shade_bytes / (kt["ms_shade"] * 1e-3) / 1e9
+    # measured DRAM bytes per traced ray (ncu, profiles/trace_traffic.json) times this run's
+    # rays per traversal launch (a launch covers every wave in flight)
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "trace_traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
-            traffic = json.load(f).get("bytes_per_launch_full_workload")
+            per_ray = json.load(f).get("bytes_per_ray_measured")
+        if per_ray:
+            rays_per_launch = (kt["rays_radiance"] + kt["rays_shadow"]) / max(1.0, kt["launches_trace"])
+            traffic = per_ray * rays_per_launch
     roof = {"bound": "hbm", "kernel": "k_trace (radiance + shadow)", "achieved": ach, "peak": hbm,
             "unit": "GB/s", "frac": ach / hbm, "traffic": traffic, "peak_source": f"{peak_kind} MEASURED_PEAKS hbm_gbs",
             "launch_ms": trace_ms_per_launch, "algorithmic_bytes_per_launch": trace_bytes_per_launch,
