@@ -42,6 +42,9 @@ static_assert(sizeof(BVH8Node) == 80, "BVH8Node must be 80 bytes");
 // 2 or 3 triangles cost more in per-lane triangle tests than they save in node visits
 // (traversal 97.5 / 107.6 ms against 83.6 ms per 16-spp step)
 constexpr int kMaxLeafPrims = 1;
+// Entries of a ray's traversal stack (shared-memory part plus local-memory part, trace.cu). A
+// scene build rejects a BVH whose depth could need more.
+constexpr int kTraversalStack = 64;
 
 }  // namespace lux
 

@@ -131,7 +131,8 @@ struct lux_ctx {
     // lanes of the wave arrays (waves in flight at once) and the lane of the last wave rendered
     int lanes = 1;
     int last_lane = 0;
-    void* wave_block = nullptr;  // the wave arrays' allocation (one of allocs)
+    void* wave_block = nullptr;  // the wave arrays' allocation (wave_block_get)
+    size_t wave_block_bytes = 0;
     // graphs: per wave size (one wave at a time), and per (waves, last wave size) of a
     // pipelined call; both hold device and page-locked host pointers of this context
     std::map<int, cudaGraphExec_t> graphs;
@@ -285,10 +286,10 @@ int make_texture(const lux_texture_desc& t, DevTex& out, int storage, TexStage& 
 // the geometry and texture threads of a scene build launch device work, so it leaves them
 // three cores: a launching thread that waits for a core stalls the device behind it.
 template <class F>
-void parallel_chunks(int n, F fn) {
+void parallel_chunks(int n, F fn, int min_chunk = 64) {
     const unsigned hw = std::thread::hardware_concurrency();
     unsigned nt = std::max(1u, std::min(hw > 4 ? hw - 3 : 1u, 64u));
-    nt = std::max(1u, std::min(nt, unsigned((n + 63) / 64)));
+    nt = std::max(1u, std::min(nt, unsigned((n + min_chunk - 1) / min_chunk)));
     std::vector<std::thread> th;
     for (unsigned t = 1; t < nt; ++t) th.emplace_back(fn, int(int64_t(n) * t / nt), int(int64_t(n) * (t + 1) / nt));
     fn(0, int(int64_t(n) / nt));
@@ -329,38 +330,47 @@ bool light_tables(const lux_scene_desc& d, const float* env, std::vector<int>& e
     emissive.clear();
     tri_prefix.assign(d.num_instances, {});
     for (int i = 0; i < d.num_instances; ++i) {
-        const lux_instance_desc& in = d.instances[i];
-        const lux_mesh_desc& m = d.meshes[in.mesh];
-        const lux_material_desc& mat = d.materials[in.material];
+        const lux_material_desc& mat = d.materials[d.instances[i].material];
         float ec = std::sqrt(mat.emission_color[0] * mat.emission_color[0] + mat.emission_color[1] * mat.emission_color[1] +
                              mat.emission_color[2] * mat.emission_color[2]);
-        bool is_em = ec * mat.emission_strength > kEPS;
-        if (!is_em) continue;  // only emissive instances' triangle tables are ever read
-        T cum = T(0);
-        std::vector<T> tp(m.num_tris);
-        for (int k = 0; k < m.num_tris; ++k) {
-            T P[3][3];
-            for (int c = 0; c < 3; ++c) {
-                const float* v = m.positions + size_t(m.indices[k * 3 + c]) * 3;
-                for (int r = 0; r < 3; ++r) {
-                    T a0 = T(in.transform[0 * 4 + r]) * T(v[0]), a1 = T(in.transform[1 * 4 + r]) * T(v[1]);
-                    T a2 = T(in.transform[2 * 4 + r]) * T(v[2]), a3 = T(in.transform[3 * 4 + r]) * T(1);
-                    P[c][r] = (a0 + a1) + (a2 + a3);
+        if (ec * mat.emission_strength > kEPS) emissive.push_back(i);  // only these tables are read
+    }
+    // each emissive instance's triangle CDF on its own thread; the instance totals then chain
+    // in instance order, as the sequential loop adds them
+    std::vector<T> inst_area(emissive.size());
+    parallel_chunks(int(emissive.size()), [&](int e0, int e1) {
+        for (int e = e0; e < e1; ++e) {
+            const int i = emissive[e];
+            const lux_instance_desc& in = d.instances[i];
+            const lux_mesh_desc& m = d.meshes[in.mesh];
+            T cum = T(0);
+            std::vector<T> tp(m.num_tris);
+            for (int k = 0; k < m.num_tris; ++k) {
+                T P[3][3];
+                for (int c = 0; c < 3; ++c) {
+                    const float* v = m.positions + size_t(m.indices[k * 3 + c]) * 3;
+                    for (int r = 0; r < 3; ++r) {
+                        T a0 = T(in.transform[0 * 4 + r]) * T(v[0]), a1 = T(in.transform[1 * 4 + r]) * T(v[1]);
+                        T a2 = T(in.transform[2 * 4 + r]) * T(v[2]), a3 = T(in.transform[3 * 4 + r]) * T(1);
+                        P[c][r] = (a0 + a1) + (a2 + a3);
+                    }
                 }
+                T u[3], v[3];
+                for (int r = 0; r < 3; ++r) {
+                    u[r] = P[1][r] - P[0][r];
+                    v[r] = P[2][r] - P[0][r];
+                }
+                T cx = u[1] * v[2] - v[1] * u[2], cy = u[2] * v[0] - v[2] * u[0], cz = u[0] * v[1] - v[0] * u[1];
+                cum += T(0.5) * std::sqrt(cx * cx + cy * cy + cz * cz);
+                tp[k] = cum;
             }
-            T u[3], v[3];
-            for (int r = 0; r < 3; ++r) {
-                u[r] = P[1][r] - P[0][r];
-                v[r] = P[2][r] - P[0][r];
-            }
-            T cx = u[1] * v[2] - v[1] * u[2], cy = u[2] * v[0] - v[2] * u[0], cz = u[0] * v[1] - v[0] * u[1];
-            cum += T(0.5) * std::sqrt(cx * cx + cy * cy + cz * cz);
-            tp[k] = cum;
+            tri_prefix[i].resize(m.num_tris);
+            for (int k = 0; k < m.num_tris; ++k) tri_prefix[i][k] = float(tp[k] / cum);
+            inst_area[e] = cum;
         }
-        tri_prefix[i].resize(m.num_tris);
-        for (int k = 0; k < m.num_tris; ++k) tri_prefix[i][k] = float(tp[k] / cum);
-        area += cum;
-        emissive.push_back(i);
+    }, 1);
+    for (size_t e = 0; e < emissive.size(); ++e) {
+        area += inst_area[e];
         ep.push_back(area);
     }
     eprefix.resize(ep.size());
@@ -690,8 +700,47 @@ int scene_create(const lux_scene_desc& d, const lux_options& o, const std::funct
     return LUX_OK;
 }
 
+// Freed wave blocks kept per device and exact size (up to kBlockKeep bytes per device) for the
+// next context of the same resolution and options: the reference re-creates its render state on
+// every camera reset, and a block of a few GB from the memory pool can cost tens of ms once the
+// pool has been churned by other sizes. Blocks come back only after the context's stream has
+// drained.
+constexpr size_t kBlockKeep = size_t(16) << 30;
+std::mutex g_block_mu;
+std::multimap<std::pair<int, size_t>, void*> g_blocks;
+std::map<int, size_t> g_block_bytes;
+
+void* wave_block_get(int dev, size_t bytes, cudaStream_t st) {
+    {
+        std::lock_guard<std::mutex> lk(g_block_mu);
+        auto it = g_blocks.find({dev, bytes});
+        if (it != g_blocks.end()) {
+            void* p = it->second;
+            g_blocks.erase(it);
+            g_block_bytes[dev] -= bytes;
+            return p;
+        }
+    }
+    void* p = nullptr;
+    if (scratch_alloc(&p, bytes, st) != cudaSuccess) return nullptr;
+    return p;
+}
+
+void wave_block_put(int dev, void* p, size_t bytes, cudaStream_t st) {
+    if (!p) return;
+    {
+        std::lock_guard<std::mutex> lk(g_block_mu);
+        if (g_block_bytes[dev] + bytes <= kBlockKeep) {
+            g_blocks.insert({{dev, bytes}, p});
+            g_block_bytes[dev] += bytes;
+            return;
+        }
+    }
+    scratch_free(p, st);
+}
+
 // The wave's arrays are carved from one allocation (each 256-byte aligned), so that a
-// context costs one cudaMalloc and one cudaFree for its whole path state.
+// context costs one allocation and one free for its whole path state.
 // Wave arrays for `lanes` waves of max_paths paths each (lane l: paths and slots
 // [l * max_paths, (l + 1) * max_paths)), counters per lane, and the table of the waves of a
 // render call. Replaces an earlier allocation (the graphs captured on it are dropped).
@@ -700,9 +749,9 @@ int alloc_wave(lux_ctx* C, int max_paths, int lanes) {
     if (C->wave_block) {
         if (C->stream) cudaStreamSynchronize(C->stream);
         C->drop_graphs();
-        scratch_free(C->wave_block, C->stream);
-        C->allocs.erase(std::remove(C->allocs.begin(), C->allocs.end(), C->wave_block), C->allocs.end());
+        wave_block_put(C->device, C->wave_block, C->wave_block_bytes, C->stream);
         C->wave_block = nullptr;
+        C->wave_block_bytes = 0;
     }
     std::memset(&W, 0, sizeof(W));
     const size_t n1 = size_t(max_paths), n = n1 * size_t(lanes);
@@ -737,9 +786,10 @@ int alloc_wave(lux_ctx* C, int max_paths, int lanes) {
         C->sort_temp_bytes = morton_sort_temp_bytes(max_paths);
         take(sort_temp, C->sort_temp_bytes);
     }
-    char* base = nullptr;
-    if (int rc = C->alloc(&base, off)) return rc;
+    char* base = static_cast<char*>(wave_block_get(C->device, off, C->stream));
+    if (!base) return fail(LUX_ERR_OOM, "device allocation of the path state failed");
     C->wave_block = base;
+    C->wave_block_bytes = off;
     for (auto& pt : parts) *pt.first = base + pt.second;
     if (C->opt.ray_sorting) C->sort_temp = sort_temp;
     W.npix = C->npix;
@@ -1519,6 +1569,7 @@ int lux_free(lux_ctx* C) {
     if (C->stream) cudaStreamSynchronize(C->stream);
     C->drop_graphs();
     for (void* p : C->allocs) scratch_free(p, C->stream);
+    wave_block_put(C->device, C->wave_block, C->wave_block_bytes, C->stream);
     pinned_put(C->h_wave_iter, sizeof(int) * 2 * size_t(C->h_cap));
     pinned_put(C->h_ctr, sizeof(WaveCounters) * size_t(C->h_cap));
     for (auto e : C->kev) cudaEventDestroy(e);

@@ -317,8 +317,10 @@ int build_geometry(const lux_scene_desc* const* scenes, int ns, const std::vecto
         for (int s = 0; s <= ns; ++s) tb[s] = int(itri[G.inst_base[s]]);
         DeviceBvh8 world;
         if (int rc = build_bvh8_device(fbox, tb, 0, true, st, world)) return rc;
+        // a node visit pushes at most two entries (the node's remaining children and a
+        // postponed triangle group), so a traversal holds at most 2 * depth + 1
         for (int s = 0; s < ns; ++s)
-            if (world.depth[s] + 4 > 16 + 48)
+            if (2 * world.depth[s] + 1 > kTraversalStack)
                 return fail(LUX_ERR_UNSUPPORTED, "acceleration structure deeper than the traversal stack");
         BVH8Node* nodes = nullptr;
         float4* fprims = nullptr;
@@ -353,8 +355,10 @@ int build_geometry(const lux_scene_desc* const* scenes, int ns, const std::vecto
         std::vector<int> tb(G.inst_base.begin(), G.inst_base.end());
         if (int rc = build_bvh8_device(ibox, tb, blas.num_nodes, true, st, tlas)) return rc;
     }
+    // two per level of either tree, and three at the instance entry (the world-level group, the
+    // rest of the TLAS leaf group and the marker)
     for (int s = 0; s < ns; ++s)
-        if (tlas.depth[s] + G.max_blas_depth[s] + 4 > 16 + 48)
+        if (2 * (tlas.depth[s] + G.max_blas_depth[s]) + 3 > kTraversalStack)
             return fail(LUX_ERR_UNSUPPORTED, "acceleration structure deeper than the traversal stack");
 
     // ---- final arrays: BLAS nodes then TLAS nodes; TLAS leaf records ----

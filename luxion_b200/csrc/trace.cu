@@ -39,6 +39,7 @@ namespace {
 
 constexpr int kShStack = 16;
 constexpr int kLocStack = 48;
+static_assert(kShStack + kLocStack == kTraversalStack, "the scene build bounds the stack by kTraversalStack");
 constexpr int kRefill = 24;
 constexpr uint32_t kTagMask = 3u << 30;
 constexpr uint32_t kTagNode = 0u;

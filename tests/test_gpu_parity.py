@@ -335,6 +335,22 @@ def test_pipelined_waves_give_identical_images(depth):
         r.close()
 
 
+def test_pipelined_call_longer_than_the_wave_table():
+    """A call of more waves than the device table of wave iterations holds (4096) runs in
+    chunks; the image equals the same samples in one wave."""
+    s = small_random_scene(seed=13, width=8, height=6, trace_depth=2)
+    base = dict(direct_light_sampling=1, env_importance_sampling=1)
+    r = lx.Renderer(s, default_options(**base, spp_per_wave=4100))
+    r.render(1, 4100)
+    ref = bits(r.image_sum())
+    r.close()
+    r = lx.Renderer(s, default_options(**base, spp_per_wave=1))
+    r.render(1, 4100)
+    assert np.array_equal(bits(r.image_sum()), ref)
+    assert r.stats()["samples"] == 4100 * 8 * 6
+    r.close()
+
+
 def test_white_furnace():
     """A smooth white metal sphere (F = 1, G ~ 1) under a constant environment of 1: every
     pixel converges to 1 (energy conservation within 1e-3)."""
