@@ -31,7 +31,7 @@ namespace lux {
 // allocations and frees are stream-ordered (no device-wide synchronisation, as cudaFree has),
 // and up to kPoolKeep bytes of freed scratch stay reserved for the next build.
 namespace {
-constexpr uint64_t kPoolKeep = uint64_t(16) << 30;
+constexpr uint64_t kPoolKeep = uint64_t(4) << 30;
 std::mutex g_pool_mu;
 std::map<int, cudaMemPool_t> g_pools;
 }  // namespace
