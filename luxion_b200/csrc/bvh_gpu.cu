@@ -169,9 +169,10 @@ struct Slot {
 
 // Chunk table of the level: chunk c covers [chunk_start[c], +kChunk) of slot chunk_slot[c]'s
 // range. One block: per-slot chunk counts, a block-wide exclusive scan, then the entries.
-__global__ void __launch_bounds__(1024) k_chunks(const int* level, int n_level, const BinNode* bn, Slot* slots,
-                                                 int* chunk_slot, int* chunk_start, int* n_chunks) {
+__global__ void __launch_bounds__(1024) k_chunks(const int* level, const int* n_level_ptr, const BinNode* bn,
+                                                 Slot* slots, int* chunk_slot, int* chunk_start, int* n_chunks) {
     __shared__ int part[1024];
+    const int n_level = *n_level_ptr;
     const int per = (n_level + 1023) / 1024;
     const int s0 = min(n_level, int(threadIdx.x) * per), s1 = min(n_level, s0 + per);
     int sum = 0;
@@ -253,7 +254,8 @@ __global__ void __launch_bounds__(kBlock) k_reduce(const float* boxes, const int
 }
 
 // Node boxes from the reductions; live axes and bin scales.
-__global__ void k_bin_setup(const int* level, int n_level, BinNode* bn, Slot* slots) {
+__global__ void k_bin_setup(const int* level, const int* n_level_ptr, BinNode* bn, Slot* slots) {
+    const int n_level = *n_level_ptr;
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n_level; s += gridDim.x * blockDim.x) {
         Slot& S = slots[s];
         BinNode& nd = bn[level[s]];
@@ -328,9 +330,10 @@ __global__ void __launch_bounds__(kBlock) k_bin(const float* boxes, const int* o
 // prefix union over lanes 0..b, those right of it a suffix union over lanes b+1..31 (empty
 // bins contribute nothing), so every candidate's cost is the host's value exactly.
 constexpr int kSplitWarps = 4;
-__global__ void __launch_bounds__(32 * kSplitWarps) k_split(const int* level, int n_level, const BinNode* bn,
+__global__ void __launch_bounds__(32 * kSplitWarps) k_split(const int* level, const int* n_level_ptr, const BinNode* bn,
                                                              Slot* slots, const unsigned* bin_cnt,
                                                              const unsigned* bin_lo, const unsigned* bin_hi) {
+    const int n_level = *n_level_ptr;
     const int lane = threadIdx.x & 31;
     for (int s = blockIdx.x * kSplitWarps + (threadIdx.x >> 5); s < n_level; s += gridDim.x * kSplitWarps) {
         Slot& S = slots[s];
@@ -449,7 +452,8 @@ __global__ void __launch_bounds__(kBlock) k_count_left(const float* boxes, const
 }
 
 // Exclusive prefix of the left counts over each node's chunks.
-__global__ void k_chunk_base(int n_level, const Slot* slots, const int* chunk_left, int* chunk_lbase) {
+__global__ void k_chunk_base(const int* n_level_ptr, const Slot* slots, const int* chunk_left, int* chunk_lbase) {
+    const int n_level = *n_level_ptr;
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n_level; s += gridDim.x * blockDim.x) {
         int run = 0;
         for (int j = 0; j < slots[s].nchunk; ++j) {
@@ -457,6 +461,25 @@ __global__ void k_chunk_base(int n_level, const Slot* slots, const int* chunk_le
             run += chunk_left[slots[s].chunk0 + j];
         }
     }
+}
+
+// Empty bins of the level's nodes: count 0, minimum keys all ones, maximum keys zero.
+__global__ void k_bin_clear(const int* n_level_ptr, unsigned* bin_cnt, unsigned* bin_lo, unsigned* bin_hi) {
+    const size_t n = size_t(*n_level_ptr) * 3 * kBins;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+        bin_cnt[i] = 0u;
+        for (int d = 0; d < 3; ++d) {
+            bin_lo[i * 3 + d] = 0xffffffffu;
+            bin_hi[i * 3 + d] = 0u;
+        }
+    }
+}
+
+// After a level: the next binary ids start past its children, and its list count is cleared
+// for the level after next (the two lists alternate).
+__global__ void k_level_advance(int* n_level_cur, int* next_id) {
+    *next_id += 2 * *n_level_cur;
+    *n_level_cur = 0;
 }
 
 // Stable partition: each chunk's primitives, in order, to the left or right part of the range.
@@ -512,9 +535,16 @@ __global__ void __launch_bounds__(kBlock) k_scatter(const float* boxes, const in
 // Children of the level's nodes: ids next_id + 2 s and + 1; leaves take their primitive's box
 // at once, small children go to the warp list (their range copied to the final order), large
 // children to the next level.
-__global__ void k_children(const float* boxes, const int* ord_next, int* ord_fin, const int* level, int n_level,
-                           BinNode* bn, const Slot* slots, int next_id, int* large_next, int* n_large_next, int* small,
-                           int* n_small) {
+// Child ids continue from *next_id (k_level_advance moves it on); ids past bn_cap set *err
+// and the level stops there.
+__global__ void k_children(const float* boxes, const int* ord_next, int* ord_fin, const int* level,
+                           const int* n_level_ptr, BinNode* bn, const Slot* slots, const int* next_id_ptr,
+                           int bn_cap, int* err, int* large_next, int* n_large_next, int* small, int* n_small) {
+    const int n_level = *n_level_ptr, next_id = *next_id_ptr;
+    if (n_level > 0 && next_id + 2 * n_level > bn_cap) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) *err = 1;
+        return;
+    }
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n_level; s += gridDim.x * blockDim.x) {
         BinNode& nd = bn[level[s]];
         const int nl = slots[s].nl;
@@ -1377,47 +1407,54 @@ int build_bvh8_device(const float* d_boxes, const std::vector<int>& tree_begin, 
     LUX_CUDA(cudaGetLastError());
     LUX_CUDA(cudaMemcpyAsync(h_ctr, ctr, 8 * sizeof(int), cudaMemcpyDeviceToHost, st));
     LUX_CUDA(cudaStreamSynchronize(st));
-    int n_level = h_ctr[0];
-    int next_id = G;
-    int cur = 0;
-    int levels = 0;
-    while (n_level > 0) {
-        if (++levels > 4 * 64 + N) return fail(LUX_ERR_UNSUPPORTED, "BVH build did not converge");
-        const int nxt = cur ^ 1;
-        if (next_id + 2 * n_level > int(bn_cap)) return fail(LUX_ERR_UNSUPPORTED, "BVH build: binary node capacity");
-        LUX_CUDA(cudaMemsetAsync(ctr + nxt, 0, sizeof(int), st));
-        const int grid_s = grid_for(n_level, 128, 4096);
-        const int grid_c = std::min(chunk_cap, 148 * 8);
-        k_chunks<<<1, 1024, 0, st>>>(large[cur], n_level, bn, slots, chunk_slot, chunk_start, ctr + 4);
-        // empty bins: count 0, minimum keys all ones, maximum keys zero
-        LUX_CUDA(cudaMemsetAsync(bin_cnt, 0, sizeof(unsigned) * size_t(n_level) * 3 * kBins, st));
-        LUX_CUDA(cudaMemsetAsync(bin_lo, 0xff, sizeof(unsigned) * size_t(n_level) * 3 * kBins * 3, st));
-        LUX_CUDA(cudaMemsetAsync(bin_hi, 0, sizeof(unsigned) * size_t(n_level) * 3 * kBins * 3, st));
-        k_reduce<<<grid_c, kBlock, 0, st>>>(d_boxes, ord[cur], large[cur], bn, slots, chunk_slot, chunk_start, ctr + 4);
-        k_bin_setup<<<grid_s, 128, 0, st>>>(large[cur], n_level, bn, slots);
-        k_bin<<<grid_c, kBlock, 0, st>>>(d_boxes, ord[cur], large[cur], bn, slots, chunk_slot, chunk_start, ctr + 4,
-                                          bin_cnt, bin_lo, bin_hi);
-        k_split<<<grid_for(n_level, kSplitWarps, 4096), 32 * kSplitWarps, 0, st>>>(large[cur], n_level, bn, slots,
-                                                                                   bin_cnt, bin_lo, bin_hi);
-        k_count_left<<<grid_c, kBlock, 0, st>>>(d_boxes, ord[cur], large[cur], bn, slots, chunk_slot, chunk_start,
-                                                 ctr + 4, chunk_left);
-        k_chunk_base<<<grid_s, 128, 0, st>>>(n_level, slots, chunk_left, chunk_lbase);
-        k_scatter<<<grid_c, kBlock, 0, st>>>(d_boxes, ord[cur], ord[nxt], large[cur], bn, slots, chunk_slot, chunk_start,
-                                              ctr + 4, chunk_lbase);
-        k_children<<<grid_s, 128, 0, st>>>(d_boxes, ord[nxt], ord_fin, large[cur], n_level, bn, slots, next_id,
-                                           large[nxt], ctr + nxt, small, ctr + 2);
-        LUX_CUDA(cudaGetLastError());
-        next_id += 2 * n_level;
+    // Binary levels of large nodes, launched in batches without reading their sizes back:
+    // every kernel takes the level's node count from ctr[cur] (the two large lists alternate),
+    // binary ids continue from ctr[3], and a level past the last has no nodes, so its kernels
+    // do nothing. One read-back per batch finds the first empty level; ctr[7] flags a binary
+    // node table too small.
+    h_ctr[3] = G;
+    LUX_CUDA(cudaMemcpyAsync(ctr + 3, h_ctr + 3, sizeof(int), cudaMemcpyHostToDevice, st));
+    int max_tree = 1;
+    for (int t = 0; t < G; ++t) max_tree = std::max(max_tree, tree_begin[t + 1] - tree_begin[t]);
+    const int grid_s = grid_for(large_cap, 128, 4096);
+    const int grid_sp = grid_for(large_cap, kSplitWarps, 4096);
+    const int grid_clear = grid_for(large_cap * 3 * kBins, 256, 148 * 16);
+    const int grid_c = std::min(chunk_cap, 148 * 8);
+    int cur = 0, levels = 0;
+    int batch = int(std::ceil(std::log2(double(max_tree) / double(kSmall) + 1.0))) + 2;
+    while (true) {
+        for (int b = 0; b < batch; ++b) {
+            if (++levels > 4 * 64 + N) return fail(LUX_ERR_UNSUPPORTED, "BVH build did not converge");
+            const int nxt = cur ^ 1;
+            k_chunks<<<1, 1024, 0, st>>>(large[cur], ctr + cur, bn, slots, chunk_slot, chunk_start, ctr + 4);
+            k_bin_clear<<<grid_clear, 256, 0, st>>>(ctr + cur, bin_cnt, bin_lo, bin_hi);
+            k_reduce<<<grid_c, kBlock, 0, st>>>(d_boxes, ord[cur], large[cur], bn, slots, chunk_slot, chunk_start,
+                                                ctr + 4);
+            k_bin_setup<<<grid_s, 128, 0, st>>>(large[cur], ctr + cur, bn, slots);
+            k_bin<<<grid_c, kBlock, 0, st>>>(d_boxes, ord[cur], large[cur], bn, slots, chunk_slot, chunk_start, ctr + 4,
+                                              bin_cnt, bin_lo, bin_hi);
+            k_split<<<grid_sp, 32 * kSplitWarps, 0, st>>>(large[cur], ctr + cur, bn, slots, bin_cnt, bin_lo, bin_hi);
+            k_count_left<<<grid_c, kBlock, 0, st>>>(d_boxes, ord[cur], large[cur], bn, slots, chunk_slot, chunk_start,
+                                                     ctr + 4, chunk_left);
+            k_chunk_base<<<grid_s, 128, 0, st>>>(ctr + cur, slots, chunk_left, chunk_lbase);
+            k_scatter<<<grid_c, kBlock, 0, st>>>(d_boxes, ord[cur], ord[nxt], large[cur], bn, slots, chunk_slot,
+                                                  chunk_start, ctr + 4, chunk_lbase);
+            k_children<<<grid_s, 128, 0, st>>>(d_boxes, ord[nxt], ord_fin, large[cur], ctr + cur, bn, slots, ctr + 3,
+                                               int(bn_cap), ctr + 7, large[nxt], ctr + nxt, small, ctr + 2);
+            k_level_advance<<<1, 1, 0, st>>>(ctr + cur, ctr + 3);
+            LUX_CUDA(cudaGetLastError());
+            cur = nxt;
+        }
         LUX_CUDA(cudaMemcpyAsync(h_ctr, ctr, 8 * sizeof(int), cudaMemcpyDeviceToHost, st));
         LUX_CUDA(cudaStreamSynchronize(st));
-        n_level = h_ctr[nxt];
-        cur = nxt;
+        if (h_ctr[7]) return fail(LUX_ERR_UNSUPPORTED, "BVH build: binary node capacity");
+        if (h_ctr[cur] == 0) break;
+        batch = 4;
     }
     // small subtrees: binary ids continue after the large levels' children
     const int n_small = h_ctr[2];
     if (n_small > 0) {
-        int* nid = ctr + 3;
-        LUX_CUDA(cudaMemcpyAsync(nid, &next_id, sizeof(int), cudaMemcpyHostToDevice, st));
+        int* nid = ctr + 3;  // the next binary id, past every large level's children
         k_small<<<grid_for(n_small, kSmallWarps, 148 * 16), 32 * kSmallWarps, 0, st>>>(d_boxes, small, ctr + 2, bn,
                                                                                         ord_fin, nid);
         LUX_CUDA(cudaGetLastError());
@@ -1466,12 +1503,10 @@ int build_bvh8_device(const float* d_boxes, const std::vector<int>& tree_begin, 
         LUX_CUDA(cudaMemcpyAsync(lvl, first, sizeof(first), cudaMemcpyHostToDevice, st));
         LUX_CUDA(cudaStreamSynchronize(st));  // `first` lives on this stack frame
     }
-    int max_tree = 1;
-    for (int t = 0; t < G; ++t) max_tree = std::max(max_tree, tree_begin[t + 1] - tree_begin[t]);
     const int max_n = int(item_cap);
     const int grid_items = grid_for(max_n, 128, 148 * 16);
     int launched = 0, L = -1;
-    int batch = int(std::ceil(0.5 * std::log2(double(max_tree) + 1.0))) + 1;
+    batch = int(std::ceil(0.5 * std::log2(double(max_tree) + 1.0))) + 1;
     while (L < 0) {
         batch = std::min(batch, kMaxLevels - launched);
         if (batch <= 0) return fail(LUX_ERR_UNSUPPORTED, "BVH build: too many 8-wide levels");
