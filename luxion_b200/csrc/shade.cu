@@ -681,6 +681,24 @@ LUX_DI PathState load_path(const DevWave& W, int pid) {
     return p;
 }
 
+// Pixel of the t-th path of a sample: 8x4 pixel tiles in row-major tile order, so that a warp's
+// 32 camera rays (and, through the order-preserving survivor queue, their later bounces) start
+// from one compact patch of the image rather than a 32x1 strip. Pixels outside the whole tiles
+// (a right margin of W % 8 columns and a bottom margin of H % 4 rows) follow in row order.
+LUX_HDI int tiled_pixel(int t, int W, int H) {
+    const int W8 = W - W % 8, H4 = H - H % 4;
+    const int a = W8 * H4;
+    if (t < a) {
+        const int tile = t >> 5, k = t & 31, tpr = W8 >> 3;
+        return ((tile / tpr) * 4 + (k >> 3)) * W + (tile % tpr) * 8 + (k & 7);
+    }
+    t -= a;
+    const int rw = W - W8;
+    if (t < rw * H4) return (t / rw) * W + W8 + t % rw;
+    t -= rw * H4;
+    return (H4 + t / W) * W + t % W;
+}
+
 // Paths [0, n) of a wave in lane `lane`: path ids and queue slots from lane * lane_stride on.
 __global__ void __launch_bounds__(kShadeBlock, 16) k_camera(DevScene S, DevWave W, DevOptions O, DevCamera C, int n,
                                                             int lane, const int* wave_iter) {
@@ -689,7 +707,7 @@ __global__ void __launch_bounds__(kShadeBlock, 16) k_camera(DevScene S, DevWave 
     const int base = lane * W.lane_stride;
     for (int local = blockIdx.x * blockDim.x + threadIdx.x; local < n; local += gridDim.x * blockDim.x) {
         const int pid = base + local;
-        int s = local / W.npix, index = local - s * W.npix;
+        int s = local / W.npix, index = tiled_pixel(local - s * W.npix, C.width, C.height);
         int iter = first_iter + s;
         int x = index % C.width, y = index / C.width;
         Rng rng = Rng::seeded(iter, index, O.trace_depth);
@@ -806,15 +824,18 @@ __global__ void __launch_bounds__(kShadeBlock, 16) k_shade(const __grid_constant
     }
 }
 
+// Path t of every sample of the wave is pixel tiled_pixel(t) (k_camera).
 __global__ void k_accumulate(const float4* __restrict__ s3, float* __restrict__ image, float* __restrict__ comp,
-                             int npix, int nsamples, int compensated) {
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+                             int width, int height, int nsamples, int compensated) {
+    const int npix = width * height;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npix; t += gridDim.x * blockDim.x) {
+        const int p = tiled_pixel(t, width, height);
         float r = image[p * 3], g = image[p * 3 + 1], b = image[p * 3 + 2];
         if (compensated) {
             // Kahan-compensated running sum (precision form)
             float cr = comp[p * 3], cg = comp[p * 3 + 1], cb = comp[p * 3 + 2];
             for (int s = 0; s < nsamples; ++s) {
-                float4 c = ld_stream(&s3[size_t(s) * npix + p]);
+                float4 c = ld_stream(&s3[size_t(s) * npix + t]);
                 float yr = c.x - cr, tr = r + yr;
                 cr = (tr - r) - yr;
                 r = tr;
@@ -830,7 +851,7 @@ __global__ void k_accumulate(const float4* __restrict__ s3, float* __restrict__ 
             comp[p * 3 + 2] = cb;
         } else {
             for (int s = 0; s < nsamples; ++s) {
-                float4 c = ld_stream(&s3[size_t(s) * npix + p]);
+                float4 c = ld_stream(&s3[size_t(s) * npix + t]);
                 r += c.x;
                 g += c.y;
                 b += c.z;
@@ -1136,7 +1157,9 @@ cudaError_t launch_accumulate(const DevWave& W, int lane, float* image, float* c
     if (lane < 0 || size_t(nsamples) * size_t(W.npix) > size_t(W.lane_stride)) return cudaErrorInvalidValue;
     int grid = std::min((W.npix + 255) / 256, 148 * 8);
     if (grid < 1) grid = 1;
-    k_accumulate<<<grid, 256, 0, st>>>(W.s3 + size_t(lane) * W.lane_stride, image, comp, W.npix, nsamples, compensated);
+    if (W.width * W.height != W.npix) return cudaErrorInvalidValue;
+    k_accumulate<<<grid, 256, 0, st>>>(W.s3 + size_t(lane) * W.lane_stride, image, comp, W.width, W.height, nsamples,
+                                       compensated);
     return cudaGetLastError();
 }
 
