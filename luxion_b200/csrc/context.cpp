@@ -700,39 +700,55 @@ int scene_create(const lux_scene_desc& d, const lux_options& o, const std::funct
     return LUX_OK;
 }
 
-// Freed wave blocks kept per device and exact size (up to kBlockKeep bytes per device) for the
-// next context of the same resolution and options: the reference re-creates its render state on
-// every camera reset, and a block of a few GB from the memory pool can cost tens of ms once the
-// pool has been churned by other sizes. Blocks come back only after the context's stream has
-// drained.
+// Freed wave blocks kept per device and size class (up to kBlockKeep bytes per device) for the
+// next context of about the same wave size: the reference re-creates its render state on every
+// camera reset, and a block of a few GB from the memory pool can cost tens of ms once the pool
+// has been churned by other sizes. Sizes are rounded up to kBlockGrain, and wave sizes cluster
+// near 8M paths whatever the resolution, so most contexts share a class. On a miss the device's
+// kept blocks go back to the pool first, where the new block can reuse their memory. Blocks come
+// back only after the context's stream has drained.
 constexpr size_t kBlockKeep = size_t(16) << 30;
+constexpr size_t kBlockGrain = size_t(128) << 20;
 std::mutex g_block_mu;
 std::multimap<std::pair<int, size_t>, void*> g_blocks;
 std::map<int, size_t> g_block_bytes;
 
+size_t block_class(size_t bytes) { return (bytes + kBlockGrain - 1) / kBlockGrain * kBlockGrain; }
+
 void* wave_block_get(int dev, size_t bytes, cudaStream_t st) {
+    const size_t cls = block_class(bytes);
     {
         std::lock_guard<std::mutex> lk(g_block_mu);
-        auto it = g_blocks.find({dev, bytes});
+        auto it = g_blocks.find({dev, cls});
         if (it != g_blocks.end()) {
             void* p = it->second;
             g_blocks.erase(it);
-            g_block_bytes[dev] -= bytes;
+            g_block_bytes[dev] -= cls;
             return p;
+        }
+        for (auto jt = g_blocks.begin(); jt != g_blocks.end();) {
+            if (jt->first.first == dev) {
+                scratch_free(jt->second, st);
+                g_block_bytes[dev] -= jt->first.second;
+                jt = g_blocks.erase(jt);
+            } else {
+                ++jt;
+            }
         }
     }
     void* p = nullptr;
-    if (scratch_alloc(&p, bytes, st) != cudaSuccess) return nullptr;
+    if (scratch_alloc(&p, cls, st) != cudaSuccess) return nullptr;
     return p;
 }
 
 void wave_block_put(int dev, void* p, size_t bytes, cudaStream_t st) {
     if (!p) return;
+    const size_t cls = block_class(bytes);
     {
         std::lock_guard<std::mutex> lk(g_block_mu);
-        if (g_block_bytes[dev] + bytes <= kBlockKeep) {
-            g_blocks.insert({{dev, bytes}, p});
-            g_block_bytes[dev] += bytes;
+        if (g_block_bytes[dev] + cls <= kBlockKeep) {
+            g_blocks.insert({{dev, cls}, p});
+            g_block_bytes[dev] += cls;
             return;
         }
     }
@@ -1350,7 +1366,9 @@ int ctx_prepare(const lux_options& o, const lux_camera_desc& cd, int scene_depth
 // Per-pixel and per-path device memory of a context (the part pathtraceInit allocates,
 // src/pathtrace/pathtrace_buffers.cu:21-140).
 int ctx_alloc(lux_ctx* C) {
-    int r = alloc_wave(C, C->spp_per_wave * C->npix, 1);
+    // the lanes of waves in flight are allocated up front: one block per context, of one size
+    // class, instead of a second, larger block at the first render of several waves
+    int r = alloc_wave(C, C->spp_per_wave * C->npix, lanes_wanted(C));
     if (!r) r = C->alloc(&C->image, size_t(C->npix) * 3);
     if (!r && C->opt.precision == LUX_PRECISION_COMPENSATED) r = C->alloc(&C->comp, size_t(C->npix) * 3);
     if (!r) r = C->alloc(&C->rgba, size_t(C->npix) * 4);
