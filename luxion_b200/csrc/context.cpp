@@ -1366,9 +1366,12 @@ int ctx_prepare(const lux_options& o, const lux_camera_desc& cd, int scene_depth
 // Per-pixel and per-path device memory of a context (the part pathtraceInit allocates,
 // src/pathtrace/pathtrace_buffers.cu:21-140).
 int ctx_alloc(lux_ctx* C) {
-    // the lanes of waves in flight are allocated up front: one block per context, of one size
-    // class, instead of a second, larger block at the first render of several waves
-    int r = alloc_wave(C, C->spp_per_wave * C->npix, lanes_wanted(C));
+    // The lanes of waves in flight are allocated up front when a wave holds few samples per
+    // pixel (half a million pixels and more), where renders of several waves are the rule: one
+    // block per context, of one size class. A smaller image's wave holds many samples per pixel,
+    // and its lanes come with the first render that needs more than one wave.
+    const int lanes = C->spp_per_wave <= 16 ? lanes_wanted(C) : 1;
+    int r = alloc_wave(C, C->spp_per_wave * C->npix, lanes);
     if (!r) r = C->alloc(&C->image, size_t(C->npix) * 3);
     if (!r && C->opt.precision == LUX_PRECISION_COMPENSATED) r = C->alloc(&C->comp, size_t(C->npix) * 3);
     if (!r) r = C->alloc(&C->rgba, size_t(C->npix) * 4);

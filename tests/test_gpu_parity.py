@@ -335,6 +335,26 @@ def test_pipelined_waves_give_identical_images(depth):
         r.close()
 
 
+def test_lanes_allocated_at_the_first_render_of_several_waves():
+    """A context whose wave holds more than 16 samples per pixel starts with one wave of state
+    and gets the lanes of waves in flight at its first render of several waves: the images of
+    one-wave and several-wave renders agree bit for bit, before and after."""
+    s = small_random_scene(seed=14, width=24, height=16, trace_depth=5)
+    base = dict(direct_light_sampling=1, env_importance_sampling=1)
+    r = lx.Renderer(s, default_options(**base, spp_per_wave=60))
+    r.render(1, 60)
+    ref = bits(r.image_sum())
+    r.close()
+    r = lx.Renderer(s, default_options(**base, spp_per_wave=17))
+    r.render(1, 10)          # one wave, in lane 0
+    r.render(11, 50)         # three waves in flight: the lanes are allocated here
+    assert np.array_equal(bits(r.image_sum()), ref)
+    r.reset()
+    r.render(1, 60)
+    assert np.array_equal(bits(r.image_sum()), ref)
+    r.close()
+
+
 def test_pipelined_call_longer_than_the_wave_table():
     """A call of more waves than the device table of wave iterations holds (4096) runs in
     chunks; the image equals the same samples in one wave."""
