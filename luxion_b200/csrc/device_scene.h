@@ -23,7 +23,8 @@ namespace lux {
 
 enum InstFlags : int { kInstHasNormals = 1, kInstHasUVs = 2, kInstAnyHit = 4 };
 
-struct DevInstance {
+// 16-byte aligned (192 bytes): traversal reads Minv as three float4.
+struct alignas(16) DevInstance {
     float M[12];      // object -> world, columns 0..3 of the 4x4 (rows 0..2)
     float Minv[12];   // world -> object
     float MinvT[12];  // inverse transpose (normal transform)

@@ -93,6 +93,19 @@ LUX_DI TRay make_ray(f3 o, f3 d) {
 // bias is folded into the per-node plane constant (visit_node), so no add removes it.
 LUX_DI float ubyte_biased(uint32_t w, int s) { return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7504u | (uint32_t(s) << 4))); }
 
+// Three-operand max / min (sm_100 and later): one instruction where two fmaxf / fminf would
+// be, with their NaN rule (a NaN operand is dropped).
+LUX_DI float max3f(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+LUX_DI float min3f(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
 // Intersect the 8 child boxes of node ni. Returns internal-child hits as a key mask
 // (bit slot ^ oct), leaf hits as a slot mask, the node's leaf-slot mask, child_base and
 // tri_base.
@@ -132,8 +145,8 @@ LUX_DI void visit_node(const uint4* __restrict__ nodes, uint32_t ni, const TRay&
               tnz = fmaf(ubyte_biased(wnz, b), az, bz);
         float tfx = fmaf(ubyte_biased(wfx, b), ax, bx), tfy = fmaf(ubyte_biased(wfy, b), ay, by),
               tfz = fmaf(ubyte_biased(wfz, b), az, bz);
-        float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
-        float tf = fminf(fminf(tfx, tfy), fminf(tfz, tmax));
+        float tn = max3f(tnx, tny, fmaxf(tnz, 0.0f));
+        float tf = min3f(tfx, tfy, fminf(tfz, tmax));
         if (tn <= tf * kWiden) hits |= 1u << s;
     }
     leafmask = w1.z & 0xffu;
@@ -334,8 +347,9 @@ struct Tracer {
             const int inst = __float_as_int(e14.w);
             if (inst != L.inst) {
                 const DevInstance& I = S.insts[inst];
-                float Minv[12];
-                for (int j = 0; j < 12; ++j) Minv[j] = __ldg(&I.Minv[j]);
+                const float4* mq = reinterpret_cast<const float4*>(I.Minv);
+                const float4 m0 = __ldg(mq), m1 = __ldg(mq + 1), m2 = __ldg(mq + 2);
+                const float Minv[12] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w, m2.x, m2.y, m2.z, m2.w};
                 L.wo = xform(Minv, L.cur.o, 1.0f);
                 L.wd = xform(Minv, L.cur.d, 0.0f);
                 L.inst = inst;
@@ -494,10 +508,93 @@ __global__ void __launch_bounds__(kTraceBlock, 7) k_trace(const __grid_constant_
     Lane L;
     bool active = false;
     bool exhausted = false;  // warp-uniform: the cursor has passed the end of the work list
+    bool pending = false;    // the lane's ray is done and its result not yet written
     int item = 0;
     // Every lane of the warp runs every phase below (lanes without a ray or without work for
     // a phase are predicated off), so the ballots see the whole warp.
     while (true) {
+        // Results of the rays that finished, written by all such lanes of the warp together
+        // (at least 32 - kRefill of them, or the last ones): a lane that finishes keeps its
+        // ray state untouched until the refill below replaces it.
+        if (pending) {
+            pending = false;
+            if (ext) {
+                uint32_t* h = A.ext_hits + size_t(item) * 5;
+                if (MODE == 2) {
+                    h[0] = __float_as_uint(L.best.inst >= 0 ? 1.0f : -1.0f);
+                    h[1] = h[2] = 0xffffffffu;
+                    h[3] = h[4] = 0u;
+                } else if (MODE == 3) {
+                    h[0] = __float_as_uint(L.best.inst >= 0 ? L.best.t : -1.0f);
+                    h[1] = uint32_t(L.best.inst);
+                    h[2] = uint32_t(L.best.prim);
+                    h[3] = uint32_t(L.work);
+                    h[4] = 0u;
+                } else {
+                    h[0] = __float_as_uint(L.best.inst >= 0 ? L.best.t : -1.0f);
+                    h[1] = uint32_t(L.best.inst);
+                    h[2] = uint32_t(L.best.prim);
+                    h[3] = __float_as_uint(L.best.inst >= 0 ? L.best.u : 0.0f);
+                    h[4] = __float_as_uint(L.best.inst >= 0 ? L.best.v : 0.0f);
+                }
+            } else if (MODE == 0) {
+                bool hit = L.best.inst >= 0;
+                st_stream(&A.W.hit[item], make_float4(hit ? L.best.t : -1.0f, L.best.u, L.best.v, __int_as_float(L.best.inst)));
+                st_stream(&A.W.hit_prim[item], L.best.prim);
+                if (hit && A.nee) {
+                    // shadow ray of the raygen program (src/optixshaders/optix_triangle.cu:82-132)
+                    f3 n = hit_world_normal(A.S, L.best.inst, L.best.prim, L.best.u, L.best.v);
+                    const f3 wo = Tracer<MODE, SINGLE>::world_o(L), wd = Tracer<MODE, SINGLE>::world_d(L);
+                    f3 hp = mk(__fadd_rn(wo.x, __fmul_rn(L.best.t, wd.x)), __fadd_rn(wo.y, __fmul_rn(L.best.t, wd.y)),
+                               __fadd_rn(wo.z, __fmul_rn(L.best.t, wd.z)));
+                    f3 so = mk(__fadd_rn(hp.x, __fmul_rn(n.x, 1e-4f)), __fadd_rn(hp.y, __fmul_rn(n.y, 1e-4f)),
+                               __fadd_rn(hp.z, __fmul_rn(n.z, 1e-4f)));
+                    // the segment of this slot: its lane, then the segment holding that lane
+                    int k = 0;
+                    if (A.G.n > 1) {
+                        const int ln = item / A.W.lane_stride;
+                        while (k + 1 < A.G.n && A.G.lane[k] != ln) ++k;
+                    }
+                    const int bk = A.G.bounce[k], lk = A.G.lane[k];
+                    int pid = ld_stream(&A.W.queue[bk & 1][item]);
+                    float4 ns = ld_stream(&A.W.s4[pid]);
+                    f3 sd;
+                    float tmax;
+                    if (A.nee == 2) {
+                        sd = mk(ns.x, ns.y, ns.z);
+                        tmax = 1e16f;
+                    } else {
+                        f3 ld = mk(__fsub_rn(ns.x, so.x), __fsub_rn(ns.y, so.y), __fsub_rn(ns.z, so.z));
+                        float dl = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(ld.x, ld.x), __fmul_rn(ld.y, ld.y)), __fmul_rn(ld.z, ld.z)));
+                        float il = __fdiv_rn(1.0f, dl);
+                        sd = mk(__fmul_rn(ld.x, il), __fmul_rn(ld.y, il), __fmul_rn(ld.z, il));
+                        tmax = __fadd_rn(__fmul_rn(dl, 1.0001f), 1e-4f);
+                    }
+                    st_stream(&A.W.sh_o[item], make_float4(so.x, so.y, so.z, tmax));
+                    st_stream(&A.W.sh_d[item], make_float4(sd.x, sd.y, sd.z, 0.0f));
+                    // append to the lane's shadow queue, aggregated over the lanes of the
+                    // warp that append to the same one
+                    const unsigned am = __match_any_sync(__activemask(), lk);
+                    int leader = __ffs(am) - 1;
+                    int b2 = 0;
+                    if (lane == leader) b2 = atomicAdd(&(A.W.ctr + lk)->shadow[bk], __popc(am));
+                    b2 = __shfl_sync(am, b2, leader);
+                    st_stream(&A.W.sh_queue[lk * A.W.lane_stride + b2 + __popc(am & ((1u << lane) - 1u))], item);
+                }
+            } else if (MODE == 1) {
+                bool hit = L.best.inst >= 0;
+                st_stream(&A.W.sh_hit[item], make_float4(hit ? L.best.t : -1.0f, L.best.u, L.best.v, __int_as_float(L.best.inst)));
+                st_stream(&A.W.sh_prim[item], L.best.prim);
+            } else if (MODE == 3) {
+                // drawBVH (src/kernels/draw_bvh.cu:33): color += count * 0.001 on every channel
+                int pid = A.W.queue[A.G.bounce[0] & 1][item];  // the heatmap traces one wave
+                float4 c = A.W.s3[pid];
+                const float h = float(L.work) * 0.001f;
+                A.W.s3[pid] = make_float4(c.x + h, c.y + h, c.z + h, c.w);
+            } else {
+                st_stream(&A.W.sh_hit[item], make_float4(L.best.inst >= 0 ? 1.0f : -1.0f, 0.0f, 0.0f, __int_as_float(-1)));
+            }
+        }
         unsigned need = __ballot_sync(FULL, !active);
         if (need && !exhausted) {
             int base = 0;
@@ -581,82 +678,7 @@ __global__ void __launch_bounds__(kTraceBlock, 7) k_trace(const __grid_constant_
             if (active && !L.done && !(L.g.y & 0xffu) && !(L.t.y & kRecMask)) T.next(L);
             if (active && L.done) {
                 active = false;
-                if (ext) {
-                    uint32_t* h = A.ext_hits + size_t(item) * 5;
-                    if (MODE == 2) {
-                        h[0] = __float_as_uint(L.best.inst >= 0 ? 1.0f : -1.0f);
-                        h[1] = h[2] = 0xffffffffu;
-                        h[3] = h[4] = 0u;
-                    } else if (MODE == 3) {
-                        h[0] = __float_as_uint(L.best.inst >= 0 ? L.best.t : -1.0f);
-                        h[1] = uint32_t(L.best.inst);
-                        h[2] = uint32_t(L.best.prim);
-                        h[3] = uint32_t(L.work);
-                        h[4] = 0u;
-                    } else {
-                        h[0] = __float_as_uint(L.best.inst >= 0 ? L.best.t : -1.0f);
-                        h[1] = uint32_t(L.best.inst);
-                        h[2] = uint32_t(L.best.prim);
-                        h[3] = __float_as_uint(L.best.inst >= 0 ? L.best.u : 0.0f);
-                        h[4] = __float_as_uint(L.best.inst >= 0 ? L.best.v : 0.0f);
-                    }
-                } else if (MODE == 0) {
-                    bool hit = L.best.inst >= 0;
-                    st_stream(&A.W.hit[item], make_float4(hit ? L.best.t : -1.0f, L.best.u, L.best.v, __int_as_float(L.best.inst)));
-                    st_stream(&A.W.hit_prim[item], L.best.prim);
-                    if (hit && A.nee) {
-                        // shadow ray of the raygen program (src/optixshaders/optix_triangle.cu:82-132)
-                        f3 n = hit_world_normal(A.S, L.best.inst, L.best.prim, L.best.u, L.best.v);
-                        const f3 wo = Tracer<MODE, SINGLE>::world_o(L), wd = Tracer<MODE, SINGLE>::world_d(L);
-                        f3 hp = mk(__fadd_rn(wo.x, __fmul_rn(L.best.t, wd.x)), __fadd_rn(wo.y, __fmul_rn(L.best.t, wd.y)),
-                                   __fadd_rn(wo.z, __fmul_rn(L.best.t, wd.z)));
-                        f3 so = mk(__fadd_rn(hp.x, __fmul_rn(n.x, 1e-4f)), __fadd_rn(hp.y, __fmul_rn(n.y, 1e-4f)),
-                                   __fadd_rn(hp.z, __fmul_rn(n.z, 1e-4f)));
-                        // the segment of this slot: its lane, then the segment holding that lane
-                        int k = 0;
-                        if (A.G.n > 1) {
-                            const int ln = item / A.W.lane_stride;
-                            while (k + 1 < A.G.n && A.G.lane[k] != ln) ++k;
-                        }
-                        const int bk = A.G.bounce[k], lk = A.G.lane[k];
-                        int pid = ld_stream(&A.W.queue[bk & 1][item]);
-                        float4 ns = ld_stream(&A.W.s4[pid]);
-                        f3 sd;
-                        float tmax;
-                        if (A.nee == 2) {
-                            sd = mk(ns.x, ns.y, ns.z);
-                            tmax = 1e16f;
-                        } else {
-                            f3 ld = mk(__fsub_rn(ns.x, so.x), __fsub_rn(ns.y, so.y), __fsub_rn(ns.z, so.z));
-                            float dl = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(ld.x, ld.x), __fmul_rn(ld.y, ld.y)), __fmul_rn(ld.z, ld.z)));
-                            float il = __fdiv_rn(1.0f, dl);
-                            sd = mk(__fmul_rn(ld.x, il), __fmul_rn(ld.y, il), __fmul_rn(ld.z, il));
-                            tmax = __fadd_rn(__fmul_rn(dl, 1.0001f), 1e-4f);
-                        }
-                        st_stream(&A.W.sh_o[item], make_float4(so.x, so.y, so.z, tmax));
-                        st_stream(&A.W.sh_d[item], make_float4(sd.x, sd.y, sd.z, 0.0f));
-                        // append to the lane's shadow queue, aggregated over the lanes of the
-                        // warp that append to the same one
-                        const unsigned am = __match_any_sync(__activemask(), lk);
-                        int leader = __ffs(am) - 1;
-                        int b2 = 0;
-                        if (lane == leader) b2 = atomicAdd(&(A.W.ctr + lk)->shadow[bk], __popc(am));
-                        b2 = __shfl_sync(am, b2, leader);
-                        st_stream(&A.W.sh_queue[lk * A.W.lane_stride + b2 + __popc(am & ((1u << lane) - 1u))], item);
-                    }
-                } else if (MODE == 1) {
-                    bool hit = L.best.inst >= 0;
-                    st_stream(&A.W.sh_hit[item], make_float4(hit ? L.best.t : -1.0f, L.best.u, L.best.v, __int_as_float(L.best.inst)));
-                    st_stream(&A.W.sh_prim[item], L.best.prim);
-                } else if (MODE == 3) {
-                    // drawBVH (src/kernels/draw_bvh.cu:33): color += count * 0.001 on every channel
-                    int pid = A.W.queue[A.G.bounce[0] & 1][item];  // the heatmap traces one wave
-                    float4 c = A.W.s3[pid];
-                    const float h = float(L.work) * 0.001f;
-                    A.W.s3[pid] = make_float4(c.x + h, c.y + h, c.z + h, c.w);
-                } else {
-                    st_stream(&A.W.sh_hit[item], make_float4(L.best.inst >= 0 ? 1.0f : -1.0f, 0.0f, 0.0f, __int_as_float(-1)));
-                }
+                pending = true;
             }
             const unsigned am = __ballot_sync(FULL, active);
             if (!am) break;
