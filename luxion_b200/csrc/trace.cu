@@ -40,7 +40,7 @@ namespace {
 constexpr int kShStack = 16;
 constexpr int kLocStack = 48;
 static_assert(kShStack + kLocStack == kTraversalStack, "the scene build bounds the stack by kTraversalStack");
-constexpr int kRefill = 24;
+constexpr int kRefill = 20;
 constexpr uint32_t kTagMask = 3u << 30;
 constexpr uint32_t kTagNode = 0u;
 constexpr uint32_t kTagTri = 1u << 30;
@@ -48,9 +48,10 @@ constexpr uint32_t kTagInst = 2u << 30;
 constexpr uint32_t kTagMarker = 3u << 30;
 constexpr uint32_t kRecMask = 0xffu;
 // fewer lanes than this with triangles to test: push the triangle groups and keep
-// traversing nodes (the postponement of Ylitie et al. 2017); 4 and a refill threshold of 24
-// lanes were the fastest of the values tried on the 1M-triangle 1080p workload
-constexpr int kPostpone = 4;
+// traversing nodes (the postponement of Ylitie et al. 2017); 6 and a refill threshold of 20
+// lanes were the fastest of the values tried on the 1M-triangle 1080p workload (3, 4 and 6;
+// 16, 20, 22, 24 and 28)
+constexpr int kPostpone = 6;
 // Slab acceptance tnear <= tfar * kWiden (tnear >= 0): a relative margin of 2^-17, far above
 // the few-ulp rounding of the plane distances.
 constexpr float kWiden = 1.0f + 1.0f / 131072.0f;
@@ -257,9 +258,23 @@ struct Lane {
     int inst;           // current instance (-1 in the TLAS)
     int inst_flags;
     uint32_t inst_prim_base;
-    int pixel, iter;    // alpha-blend hash key
+    int key;            // path id (wave rays) or pixel (rays given directly): the alpha-blend
+                        // hash key, resolved only when an alpha-blended instance is tested
     int work;           // BVH heatmap (mode 3): node visits + triangle tests
     bool done;
+};
+
+struct TraceArgs {
+    DevScene S;
+    DevWave W;
+    Segs G;      // the (lane, bounce) segments of the launch
+    int mode;    // 0 radiance, 1 DL shadow, 2 env shadow, 3 BVH heatmap of radiance rays
+    int nee;     // radiance pass: 0 none, 1 DL, 2 env
+    const float* ext_rays;  // lux_trace_rays: rays given directly (n * 8 floats)
+    uint32_t* ext_hits;     // and hits written directly (n * 5 words)
+    int ext_n;
+    int ext_iter;
+    int* ext_fetch;
 };
 
 template <int MODE, bool SINGLE>
@@ -269,6 +284,7 @@ struct Tracer {
     uint2 loc[kLocStack];
     int tid;
     int* err;
+    const TraceArgs& A;  // the launch's arguments, in parameter space like S
 
     LUX_DI void push(Lane& L, uint2 e) {
         if (L.sp < kShStack) sh[L.sp][tid] = e;
@@ -362,7 +378,12 @@ struct Tracer {
         if (!(t <= L.tmax)) return;
         if (MODE != 2 && !better(t, L.inst, prim, L.best)) return;
         if (L.inst_flags & kInstAnyHit) {
-            if (!alpha_accept(S, S.insts[L.inst], L.inst, prim, u, v, world_d(L), L.pixel, L.iter)) return;
+            int pixel = L.key, iter = A.ext_iter;
+            if (A.ext_rays == nullptr) {  // key = path id: pixel in s2.w, iteration in s3.w
+                pixel = __float_as_int(A.W.s2[L.key].w);
+                iter = __float_as_int(A.W.s3[L.key].w);
+            }
+            if (!alpha_accept(S, S.insts[L.inst], L.inst, prim, u, v, world_d(L), pixel, iter)) return;
         }
         L.best.t = t;
         L.best.inst = L.inst;
@@ -419,18 +440,6 @@ struct Tracer {
     }
 };
 
-struct TraceArgs {
-    DevScene S;
-    DevWave W;
-    Segs G;      // the (lane, bounce) segments of the launch
-    int mode;    // 0 radiance, 1 DL shadow, 2 env shadow, 3 BVH heatmap of radiance rays
-    int nee;     // radiance pass: 0 none, 1 DL, 2 env
-    const float* ext_rays;  // lux_trace_rays: rays given directly (n * 8 floats)
-    uint32_t* ext_hits;     // and hits written directly (n * 5 words)
-    int ext_n;
-    int ext_iter;
-    int* ext_fetch;
-};
 
 // World normal of a radiance hit as the closest-hit program computes it
 // (src/optixshaders/optix_triangle.cu:170-192,224): interpolated vertex normals when the
@@ -488,7 +497,7 @@ __global__ void __launch_bounds__(kTraceBlock, 7) k_trace(const __grid_constant_
         }
     }
     __syncthreads();
-    Tracer<MODE, SINGLE> T{A.S, stack, {}, int(threadIdx.x), &(A.W.ctr + A.G.lane[0])->error};
+    Tracer<MODE, SINGLE> T{A.S, stack, {}, int(threadIdx.x), &(A.W.ctr + A.G.lane[0])->error, A};
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     int total;
@@ -608,15 +617,13 @@ __global__ void __launch_bounds__(kTraceBlock, 7) k_trace(const __grid_constant_
                     f3 o, d;
                     float tmax;
                     uint32_t root = A.S.tlas_root;
-                    L.pixel = 0;
-                    L.iter = 0;
+                    L.key = 0;
                     if (ext) {
                         const float* ry = A.ext_rays + size_t(r) * 8;
                         o = mk(ry[0], ry[1], ry[2]);
                         d = mk(ry[4], ry[5], ry[6]);
                         tmax = MODE == 1 ? ry[3] : 1e16f;
-                        L.pixel = __float_as_int(ry[7]);
-                        L.iter = A.ext_iter;
+                        L.key = __float_as_int(ry[7]);
                     } else if (MODE == 0 || MODE == 3) {
                         int k = 0;
                         while (k + 1 < A.G.n && r >= seg_first[k + 1]) ++k;
@@ -626,8 +633,7 @@ __global__ void __launch_bounds__(kTraceBlock, 7) k_trace(const __grid_constant_
                         o = mk(a.x, a.y, a.z);
                         d = mk(b.x, b.y, b.z);
                         tmax = 1e16f;
-                        L.pixel = __float_as_int(ld_stream(&A.W.s2[pid]).w);
-                        L.iter = __float_as_int(ld_stream(&A.W.s3[pid]).w);
+                        L.key = pid;
                         if (A.W.path_job) root = A.W.jobs[A.W.path_job[pid]].tlas_root;
                     } else {
                         int k = 0;
@@ -639,8 +645,7 @@ __global__ void __launch_bounds__(kTraceBlock, 7) k_trace(const __grid_constant_
                         d = mk(b.x, b.y, b.z);
                         tmax = a.w;
                         int pid = ld_stream(&A.W.queue[A.G.bounce[k] & 1][slot]);
-                        L.pixel = __float_as_int(ld_stream(&A.W.s2[pid]).w);
-                        L.iter = __float_as_int(ld_stream(&A.W.s3[pid]).w);
+                        L.key = pid;
                         if (A.W.path_job) root = A.W.jobs[A.W.path_job[pid]].tlas_root;
                     }
                     T.start(L, o, d, tmax, root);
