@@ -667,9 +667,10 @@ int check_options_and_device(const lux_options& o) {
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(LUX_ERR_NO_DEVICE, "no CUDA device");
     if (o.device < 0 || o.device >= ndev) return fail(LUX_ERR_INVALID, "device ordinal out of range");
-    cudaDeviceProp prop;
-    cudaGetDeviceProperties(&prop, o.device);
-    if (prop.major < 10) return fail(LUX_ERR_NO_DEVICE, "an sm_100 device is required");
+    // one attribute, not cudaGetDeviceProperties, which fills every field of the struct
+    int major = 0;
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, o.device);
+    if (major < 10) return fail(LUX_ERR_NO_DEVICE, "an sm_100 device is required");
     LUX_CUDA(cudaSetDevice(o.device));
     return LUX_OK;
 }
@@ -1366,11 +1367,13 @@ int ctx_prepare(const lux_options& o, const lux_camera_desc& cd, int scene_depth
 // Per-pixel and per-path device memory of a context (the part pathtraceInit allocates,
 // src/pathtrace/pathtrace_buffers.cu:21-140).
 int ctx_alloc(lux_ctx* C) {
-    // The lanes of waves in flight are allocated up front when a wave holds few samples per
-    // pixel (half a million pixels and more), where renders of several waves are the rule: one
-    // block per context, of one size class. A smaller image's wave holds many samples per pixel,
-    // and its lanes come with the first render that needs more than one wave.
-    const int lanes = C->spp_per_wave <= 16 ? lanes_wanted(C) : 1;
+    // The lanes of waves in flight come with the context, in one block. A wave holds about 8M
+    // paths whatever the resolution, so most contexts ask for one size class, and a freed
+    // context's block serves the next. (Giving a small image one lane here and its other lanes
+    // at its first render of several waves made two classes alternate in a stream of mixed
+    // sizes: each miss sent the kept blocks back to the pool, and a sequence of 64 plain renders
+    // of mixed sizes took 3.7 s instead of 1.4.)
+    const int lanes = lanes_wanted(C);
     int r = alloc_wave(C, C->spp_per_wave * C->npix, lanes);
     if (!r) r = C->alloc(&C->image, size_t(C->npix) * 3);
     if (!r && C->opt.precision == LUX_PRECISION_COMPENSATED) r = C->alloc(&C->comp, size_t(C->npix) * 3);

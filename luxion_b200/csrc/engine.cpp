@@ -274,9 +274,10 @@ int lux_engine_create(const lux_scene_desc* const* scenes, int num_scenes, const
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(LUX_ERR_NO_DEVICE, "no CUDA device");
     if (o.device < 0 || o.device >= ndev) return fail(LUX_ERR_INVALID, "device ordinal out of range");
-    cudaDeviceProp prop;
-    cudaGetDeviceProperties(&prop, o.device);
-    if (prop.major < 10) return fail(LUX_ERR_NO_DEVICE, "an sm_100 device is required");
+    // one attribute, not cudaGetDeviceProperties, which fills every field of the struct
+    int major = 0;
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, o.device);
+    if (major < 10) return fail(LUX_ERR_NO_DEVICE, "an sm_100 device is required");
     LUX_CUDA(cudaSetDevice(o.device));
 
     lux_engine* E = new lux_engine();

@@ -407,10 +407,10 @@ def test_pipelined_waves_give_identical_images(depth):
         r.close()
 
 
-def test_lanes_allocated_at_the_first_render_of_several_waves():
-    """A context whose wave holds more than 16 samples per pixel starts with one wave of state
-    and gets the lanes of waves in flight at its first render of several waves: the images of
-    one-wave and several-wave renders agree bit for bit, before and after."""
+def test_many_spp_waves_split_across_calls():
+    """A context whose wave holds more than 16 samples per pixel: a call of one wave, then a
+    call of three waves in flight, then a reset and one call of four, all agree bit for bit
+    with one 60-spp wave."""
     s = small_random_scene(seed=14, width=24, height=16, trace_depth=5)
     base = dict(direct_light_sampling=1, env_importance_sampling=1)
     r = lx.Renderer(s, default_options(**base, spp_per_wave=60))
@@ -419,7 +419,7 @@ def test_lanes_allocated_at_the_first_render_of_several_waves():
     r.close()
     r = lx.Renderer(s, default_options(**base, spp_per_wave=17))
     r.render(1, 10)          # one wave, in lane 0
-    r.render(11, 50)         # three waves in flight: the lanes are allocated here
+    r.render(11, 50)         # three waves in flight
     assert np.array_equal(bits(r.image_sum()), ref)
     r.reset()
     r.render(1, 60)
