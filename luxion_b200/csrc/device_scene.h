@@ -190,9 +190,9 @@ struct DevWave {
     int* queue[2];
     float4* hit;      // per slot: t, u, v, instance (int bits)
     int* hit_prim;    // per slot
-    float4* sh_o;     // per slot: shadow origin, tmax
-    float4* sh_d;     // per slot: shadow direction
-    int* sh_queue;    // slots with a shadow ray
+    float4* sh_o;     // per shadow-queue position: shadow origin, tmax
+    float4* sh_d;     // per shadow-queue position: shadow direction
+    int* sh_queue;    // per shadow-queue position: the slot the shadow ray belongs to
     float4* sh_hit;   // per slot: DL hit t, u, v, instance; env: occlusion in .x
     int* sh_prim;
     uint32_t* keys;   // Morton keys (ray sorting)

@@ -41,6 +41,8 @@ constexpr int kShStack = 16;
 constexpr int kLocStack = 48;
 static_assert(kShStack + kLocStack == kTraversalStack, "the scene build bounds the stack by kTraversalStack");
 constexpr int kRefill = 20;
+// environment occlusion rays (any hit, mode 2) refill below this many traversing lanes
+constexpr int kRefillOcclusion = 24;
 constexpr uint32_t kTagMask = 3u << 30;
 constexpr uint32_t kTagNode = 0u;
 constexpr uint32_t kTagTri = 1u << 30;
@@ -50,7 +52,7 @@ constexpr uint32_t kRecMask = 0xffu;
 // fewer lanes than this with triangles to test: push the triangle groups and keep
 // traversing nodes (the postponement of Ylitie et al. 2017); 6 and a refill threshold of 20
 // lanes were the fastest of the values tried on the 1M-triangle 1080p workload (3, 4 and 6;
-// 16, 20, 22, 24 and 28)
+// 16, 20, 22, 24 and 28), and 24 for the occlusion rays (16, 20 and 24)
 constexpr int kPostpone = 6;
 // Slab acceptance tnear <= tfar * kWiden (tnear >= 0): a relative margin of 2^-17, far above
 // the few-ulp rounding of the plane distances.
@@ -579,16 +581,19 @@ __global__ void __launch_bounds__(kTraceBlock, 7) k_trace(const __grid_constant_
                         sd = mk(__fmul_rn(ld.x, il), __fmul_rn(ld.y, il), __fmul_rn(ld.z, il));
                         tmax = __fadd_rn(__fmul_rn(dl, 1.0001f), 1e-4f);
                     }
-                    st_stream(&A.W.sh_o[item], make_float4(so.x, so.y, so.z, tmax));
-                    st_stream(&A.W.sh_d[item], make_float4(sd.x, sd.y, sd.z, 0.0f));
                     // append to the lane's shadow queue, aggregated over the lanes of the
-                    // warp that append to the same one
+                    // warp that append to the same one; the ray is stored at its queue
+                    // position, beside the slot it belongs to, so the occlusion launch reads
+                    // rays contiguously and without first reading the slot
                     const unsigned am = __match_any_sync(__activemask(), lk);
                     int leader = __ffs(am) - 1;
                     int b2 = 0;
                     if (lane == leader) b2 = atomicAdd(&(A.W.ctr + lk)->shadow[bk], __popc(am));
                     b2 = __shfl_sync(am, b2, leader);
-                    st_stream(&A.W.sh_queue[lk * A.W.lane_stride + b2 + __popc(am & ((1u << lane) - 1u))], item);
+                    const size_t q = size_t(lk) * A.W.lane_stride + b2 + __popc(am & ((1u << lane) - 1u));
+                    st_stream(&A.W.sh_o[q], make_float4(so.x, so.y, so.z, tmax));
+                    st_stream(&A.W.sh_d[q], make_float4(sd.x, sd.y, sd.z, 0.0f));
+                    st_stream(&A.W.sh_queue[q], item);
                 }
             } else if (MODE == 1) {
                 bool hit = L.best.inst >= 0;
@@ -638,9 +643,10 @@ __global__ void __launch_bounds__(kTraceBlock, 7) k_trace(const __grid_constant_
                     } else {
                         int k = 0;
                         while (k + 1 < A.G.n && r >= seg_first[k + 1]) ++k;
-                        int slot = ld_stream(&A.W.sh_queue[A.G.lane[k] * A.W.lane_stride + (r - seg_first[k])]);
+                        const size_t q = size_t(A.G.lane[k]) * A.W.lane_stride + (r - seg_first[k]);
+                        int slot = ld_stream(&A.W.sh_queue[q]);
                         item = slot;
-                        float4 a = ld_stream(&A.W.sh_o[slot]), b = ld_stream(&A.W.sh_d[slot]);
+                        float4 a = ld_stream(&A.W.sh_o[q]), b = ld_stream(&A.W.sh_d[q]);
                         o = mk(a.x, a.y, a.z);
                         d = mk(b.x, b.y, b.z);
                         tmax = a.w;
@@ -687,7 +693,7 @@ __global__ void __launch_bounds__(kTraceBlock, 7) k_trace(const __grid_constant_
             }
             const unsigned am = __ballot_sync(FULL, active);
             if (!am) break;
-            if (__popc(am) < kRefill && !exhausted) break;
+            if (__popc(am) < (MODE == 2 ? kRefillOcclusion : kRefill) && !exhausted) break;
         }
     }
 }
