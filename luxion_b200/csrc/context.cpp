@@ -705,9 +705,11 @@ int scene_create(const lux_scene_desc& d, const lux_options& o, const std::funct
 // next context of about the same wave size: the reference re-creates its render state on every
 // camera reset, and a block of a few GB from the memory pool can cost tens of ms once the pool
 // has been churned by other sizes. Sizes are rounded up to kBlockGrain, and wave sizes cluster
-// near 8M paths whatever the resolution, so most contexts share a class. On a miss the device's
-// kept blocks go back to the pool first, where the new block can reuse their memory. Blocks come
-// back only after the context's stream has drained.
+// near 8M paths whatever the resolution, so most contexts share a class or two (a 1080p wave of
+// 4 spp is 8.29M paths, one of 512x512 at 32 spp 8.39M: classes 41 and 42). A request takes the
+// smallest kept block of its class or up to a quarter larger, so neighbouring classes share
+// blocks. On a miss the device's kept blocks go back to the pool first, where the new block can
+// reuse their memory. Blocks come back only after the context's stream has drained.
 constexpr size_t kBlockKeep = size_t(16) << 30;
 constexpr size_t kBlockGrain = size_t(128) << 20;
 std::mutex g_block_mu;
@@ -716,15 +718,17 @@ std::map<int, size_t> g_block_bytes;
 
 size_t block_class(size_t bytes) { return (bytes + kBlockGrain - 1) / kBlockGrain * kBlockGrain; }
 
-void* wave_block_get(int dev, size_t bytes, cudaStream_t st) {
+// *cap receives the capacity of the block returned (its class), which wave_block_put takes back.
+void* wave_block_get(int dev, size_t bytes, cudaStream_t st, size_t* cap) {
     const size_t cls = block_class(bytes);
     {
         std::lock_guard<std::mutex> lk(g_block_mu);
-        auto it = g_blocks.find({dev, cls});
-        if (it != g_blocks.end()) {
+        auto it = g_blocks.lower_bound({dev, cls});
+        if (it != g_blocks.end() && it->first.first == dev && it->first.second <= cls + cls / 4) {
             void* p = it->second;
+            *cap = it->first.second;
+            g_block_bytes[dev] -= it->first.second;
             g_blocks.erase(it);
-            g_block_bytes[dev] -= cls;
             return p;
         }
         for (auto jt = g_blocks.begin(); jt != g_blocks.end();) {
@@ -739,6 +743,7 @@ void* wave_block_get(int dev, size_t bytes, cudaStream_t st) {
     }
     void* p = nullptr;
     if (scratch_alloc(&p, cls, st) != cudaSuccess) return nullptr;
+    *cap = cls;
     return p;
 }
 
@@ -803,10 +808,11 @@ int alloc_wave(lux_ctx* C, int max_paths, int lanes) {
         C->sort_temp_bytes = morton_sort_temp_bytes(max_paths);
         take(sort_temp, C->sort_temp_bytes);
     }
-    char* base = static_cast<char*>(wave_block_get(C->device, off, C->stream));
+    size_t cap = 0;
+    char* base = static_cast<char*>(wave_block_get(C->device, off, C->stream, &cap));
     if (!base) return fail(LUX_ERR_OOM, "device allocation of the path state failed");
     C->wave_block = base;
-    C->wave_block_bytes = off;
+    C->wave_block_bytes = cap;
     for (auto& pt : parts) *pt.first = base + pt.second;
     if (C->opt.ray_sorting) C->sort_temp = sort_temp;
     W.npix = C->npix;
