@@ -1,7 +1,7 @@
 """Parity of the CUDA path (through the C-ABI) with the CPU oracle and with the golden vectors
 of the reference's own sources.
 
-Tolerances (BASELINE north star): integer and index outputs -- RNG streams, CDF tables and
+Tolerances: integer and index outputs -- RNG streams, CDF tables and
 sample indices, hit instance/primitive ids, Morton keys, survivor sets -- bit-exact; hit
 distances and barycentrics bit-exact as well (the triangle test is evaluated with the same
 single-rounded operations); FP32 radiance within 1e-3 relative on >= 99.9% of pixels with
