@@ -46,6 +46,7 @@ def serve_engine(engine: Engine, requests: List[dict], keep_images: bool = False
                 time.sleep(wait / 1000.0)
             continue
         if done:
+            found = 0  # the step finished `done` jobs: stop looking once they are all collected
             for jid in list(live):
                 s = engine.status(jid)
                 if s["state"] == 2:  # LUX_JOB_DONE
@@ -56,6 +57,9 @@ def serve_engine(engine: Engine, requests: List[dict], keep_images: bool = False
                         images[i] = img
                     samples += reqs[i]["camera"].width * reqs[i]["camera"].height * reqs[i]["spp"]
                     engine.release(jid)
+                    found += 1
+                    if found == done:
+                        break
     wall = engine.clock_ms() - t0
     st = engine.stats()
     out = percentiles(lat)
