@@ -418,7 +418,7 @@ enum { LUX_JOB_QUEUED = 0, LUX_JOB_ACTIVE = 1, LUX_JOB_DONE = 2, LUX_JOB_RELEASE
 
 typedef struct lux_job_status {
     int32_t state;            /* LUX_JOB_*                                                     */
-    int32_t spp_done;         /* samples accumulated so far (a progressive result)             */
+    int32_t spp_done;         /* samples accumulated so far, as an image read now holds them    */
     int32_t spp;
     int32_t waves;            /* waves the job took part in                                     */
     double t_submit_ms, t_admit_ms, t_done_ms;   /* engine clock (ms since creation)            */
@@ -444,7 +444,11 @@ int lux_engine_submit(lux_engine* e, const lux_job_desc* job, int* job_id);
  * may be NULL). The first waves (the autotuning ones) run one whole wave per call; after them
  * up to four waves are in flight: a call starts a new wave when a lane is free and there is
  * work, advances every wave in flight by three bounces, and accumulates the waves that are
- * through, in the order they started. *idle is set to 1 when there was nothing to render. */
+ * through, in the order they started. Such a call returns while its step runs on the device,
+ * after finishing the step before it: the jobs a step completes are reported (*done_jobs,
+ * LUX_JOB_DONE) by the next call, and a job's spp_done counts the samples whose accumulation
+ * has been enqueued, which an image read back now holds. *idle is set to 1 when there was
+ * nothing to render and nothing left to report. */
 int lux_engine_step(lux_engine* e, int* done_jobs, int* idle);
 /* Step until every submitted job is done. */
 int lux_engine_run(lux_engine* e);

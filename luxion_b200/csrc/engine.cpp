@@ -37,6 +37,7 @@ struct EngineJob {
     int state = LUX_JOB_QUEUED;
     int slot = -1;  // row of the device job table while admitted
     int spp_sched = 0, spp_done = 0, waves = 0;
+    int spp_final = 0;  // samples whose accumulation has completed on the device
     int depth = 0;
     int npix = 0;
     size_t bytes = 0;
@@ -88,9 +89,11 @@ struct lux_engine {
     DevJob* jobs_d = nullptr;
     DevJob* jobs_h = nullptr;     // pinned mirror, one row per slot
     DevSegment* segs_d = nullptr; // per lane, kMaxSegments each
-    DevSegment* segs_h = nullptr; // pinned, per lane
-    int* hdr_h = nullptr;         // pinned, 4 ints per lane
-    WaveCounters* ctr_h = nullptr;  // pinned, per lane
+    // pinned, per lane and twice (by step parity): a wave planned while the step before is
+    // still on the device must not overwrite a table whose copy that step has not yet made
+    DevSegment* segs_h = nullptr; // kMaxSegments per lane
+    int* hdr_h = nullptr;         // 4 ints per lane
+    WaveCounters* ctr_h = nullptr;  // pinned, per lane, twice (by step parity)
     int lanes = kEngineLanes;
     std::deque<Flight> flight;    // waves in flight, in start order
     int max_jobs = 0;
@@ -100,6 +103,14 @@ struct lux_engine {
     std::vector<int> active;
     std::map<std::tuple<int, int, int>, cudaGraphExec_t> graphs;  // (depth, wave size, trace grid)
     cudaEvent_t ev[2] = {nullptr, nullptr};
+    // Pipelined steps: a call enqueues its step and then finishes the step before it, so the
+    // device runs one step while the host finishes the last and serves finished jobs.
+    cudaEvent_t step_ev[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // (start, end) by parity
+    int step_par = 0;
+    bool pend_valid = false;  // a step is enqueued whose accumulated waves await bookkeeping
+    int pend_par = 0;
+    std::vector<Flight> pend_fin;
+    cudaStream_t copy_stream = nullptr;  // read-back of finished jobs' images
     // autotuning of (wave size, trace grid) on the first waves
     std::vector<std::pair<int, int>> tune_cands;
     std::vector<double> tune_cost;  // device ms per path of each candidate's wave
@@ -360,13 +371,18 @@ int lux_engine_create(const lux_scene_desc* const* scenes, int num_scenes, const
     W.max_paths = E->paths_alloc;
     W.lane_stride = E->paths_alloc;
     if (cudaMallocHost(&E->jobs_h, sizeof(DevJob) * E->max_jobs) != cudaSuccess ||
-        cudaMallocHost(&E->segs_h, sizeof(DevSegment) * kMaxSegments * L) != cudaSuccess ||
-        cudaMallocHost(&E->hdr_h, sizeof(int) * 4 * L) != cudaSuccess ||
-        cudaMallocHost(&E->ctr_h, sizeof(WaveCounters) * L) != cudaSuccess)
+        cudaMallocHost(&E->segs_h, sizeof(DevSegment) * kMaxSegments * 2 * L) != cudaSuccess ||
+        cudaMallocHost(&E->hdr_h, sizeof(int) * 4 * 2 * L) != cudaSuccess ||
+        cudaMallocHost(&E->ctr_h, sizeof(WaveCounters) * 2 * L) != cudaSuccess)
         return bail(fail(LUX_ERR_OOM, "pinned host allocation failed"));
     for (int s = E->max_jobs - 1; s >= 0; --s) E->free_slots.push_back(s);
     cudaEventCreate(&E->ev[0]);
     cudaEventCreate(&E->ev[1]);
+    for (auto& pe : E->step_ev)
+        for (cudaEvent_t& e : pe)
+            if (cudaEventCreate(&e) != cudaSuccess) return bail(fail(LUX_ERR_CUDA, "event creation failed"));
+    if (cudaStreamCreateWithFlags(&E->copy_stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(LUX_ERR_CUDA, "stream creation failed"));
     // occupancy queries happen here, never inside a stream capture
     for (int m = 0; m < 3; ++m) trace_grid_blocks(m, E->S.single_level != 0);
     shade_grid_blocks();
@@ -453,8 +469,9 @@ int plan_next(lux_engine* E, int lane, int& wave_paths, int& depth, int& path0,
         nsegs = lux_plan_wave(np.data(), rem.data(), nj, wave_paths, kMaxSegments, take.data());
     }
     if (nsegs <= 0) return 0;
-    DevSegment* segs_h = E->segs_h + size_t(lane) * kMaxSegments;
-    int* hdr_h = E->hdr_h + size_t(lane) * 4;
+    const size_t buf = size_t(E->step_par) * E->lanes + lane;
+    DevSegment* segs_h = E->segs_h + buf * kMaxSegments;
+    int* hdr_h = E->hdr_h + buf * 4;
     path0 = 0;
     depth = 0;
     part.clear();
@@ -480,8 +497,18 @@ int plan_next(lux_engine* E, int lane, int& wave_paths, int& depth, int& path0,
     return k;
 }
 
-// Bookkeeping of a wave that has been accumulated (its counters copied to c): rays, samples,
-// and the jobs it completed.
+// Samples a wave adds to its jobs, counted when its accumulation is enqueued: an image read
+// back in stream order (which waits for everything enqueued) then holds spp_done samples.
+void count_wave(lux_engine* E, const std::vector<std::pair<int, int>>& part) {
+    for (auto& pr : part) {
+        EngineJob& j = E->jobs[pr.first];
+        j.spp_done += pr.second;
+        j.waves += 1;
+    }
+}
+
+// Bookkeeping of a wave whose accumulation has completed on the device (its counters copied to
+// c): rays, samples, and the jobs it completed (every sample's accumulation completed).
 int finish_wave(lux_engine* E, const WaveCounters& c, int depth, int paths, const std::vector<std::pair<int, int>>& part) {
     if (c.error) return fail(LUX_ERR_UNSUPPORTED, "traversal stack overflow");
     const double t = now_ms(E->t0);
@@ -493,9 +520,8 @@ int finish_wave(lux_engine* E, const WaveCounters& c, int depth, int paths, cons
     int done = 0;
     for (auto& pr : part) {
         EngineJob& j = E->jobs[pr.first];
-        j.spp_done += pr.second;
-        j.waves += 1;
-        if (j.spp_done == j.desc.spp) {
+        j.spp_final += pr.second;
+        if (j.state == LUX_JOB_ACTIVE && j.spp_final == j.desc.spp) {
             j.state = LUX_JOB_DONE;
             j.t_done = t;
             ++done;
@@ -556,9 +582,31 @@ int step_one_wave(lux_engine* E, bool tuning, int* done_jobs, int* idle) {
             E->trace_blocks = E->tune_cands[best].second;
         }
     }
+    count_wave(E, part);
     const int done = finish_wave(E, *E->ctr_h, depth, path0, part);
     if (done < 0) return done;
     if (done_jobs) *done_jobs = done;
+    return LUX_OK;
+}
+
+// Bookkeeping of the pipelined step enqueued last: waits for its end event, then counts its
+// device time and finishes the waves it accumulated (their counters in its parity's buffers).
+int finish_pending(lux_engine* E, int* done) {
+    *done = 0;
+    if (!E->pend_valid) return LUX_OK;
+    E->pend_valid = false;
+    const int p = E->pend_par;
+    LUX_CUDA(cudaEventSynchronize(E->step_ev[p][1]));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, E->step_ev[p][0], E->step_ev[p][1]);
+    E->stats.ms_device += ms;
+    std::vector<Flight> fin = std::move(E->pend_fin);
+    E->pend_fin.clear();
+    for (const Flight& f : fin) {
+        const int d = finish_wave(E, E->ctr_h[size_t(p) * E->lanes + f.lane], f.depth, f.paths, f.part);
+        if (d < 0) return d;
+        *done += d;
+    }
     return LUX_OK;
 }
 
@@ -589,10 +637,16 @@ int step_pipelined(lux_engine* E, int* done_jobs, int* idle) {
         }
     }
     if (E->flight.empty()) {
-        if (idle) *idle = 1;
+        // nothing in flight: the step enqueued last, if any, is the last to finish
+        int done = 0;
+        if (int rc = finish_pending(E, &done)) return rc;
+        if (done_jobs) *done_jobs = done;
+        if (idle && done == 0) *idle = 1;
         return LUX_OK;
     }
-    LUX_CUDA(cudaEventRecord(E->ev[0], st));
+    const int par = E->step_par;
+    E->step_par ^= 1;
+    LUX_CUDA(cudaEventRecord(E->step_ev[par][0], st));
     for (int s = 0; s < kStepBounces; ++s) {
         Segs G{};
         for (const Flight& f : E->flight) {
@@ -614,20 +668,18 @@ int step_pipelined(lux_engine* E, int* done_jobs, int* idle) {
         Flight f = std::move(E->flight.front());
         E->flight.pop_front();
         LUX_CUDA(launch_accumulate_jobs(lane_view(E, f.lane), E->opt.precision == LUX_PRECISION_COMPENSATED, f.lane, st));
-        LUX_CUDA(cudaMemcpyAsync(E->ctr_h + f.lane, E->W.ctr + f.lane, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st));
+        LUX_CUDA(cudaMemcpyAsync(E->ctr_h + size_t(par) * E->lanes + f.lane, E->W.ctr + f.lane, sizeof(WaveCounters),
+                                 cudaMemcpyDeviceToHost, st));
+        count_wave(E, f.part);
         fin.push_back(std::move(f));
     }
-    LUX_CUDA(cudaEventRecord(E->ev[1], st));
-    LUX_CUDA(cudaStreamSynchronize(st));
-    float ms = 0;
-    cudaEventElapsedTime(&ms, E->ev[0], E->ev[1]);
-    E->stats.ms_device += ms;
+    LUX_CUDA(cudaEventRecord(E->step_ev[par][1], st));
+    // this step runs on the device while the one before it is finished here
     int done = 0;
-    for (const Flight& f : fin) {
-        const int d = finish_wave(E, E->ctr_h[f.lane], f.depth, f.paths, f.part);
-        if (d < 0) return d;
-        done += d;
-    }
+    if (int rc = finish_pending(E, &done)) return rc;
+    E->pend_valid = true;
+    E->pend_par = par;
+    E->pend_fin = std::move(fin);
     if (done_jobs) *done_jobs = done;
     return LUX_OK;
 }
@@ -690,6 +742,13 @@ int lux_engine_copy_image(lux_engine* E, int id, float* rgb) {
         return LUX_OK;
     }
     LUX_CUDA(cudaSetDevice(E->device));
+    if (j.state == LUX_JOB_DONE && E->copy_stream) {
+        // its last accumulation is complete (the step's end event was waited for): read it back
+        // on the side stream, without waiting for the step now running
+        LUX_CUDA(cudaMemcpyAsync(rgb, j.image, bytes, cudaMemcpyDeviceToHost, E->copy_stream));
+        LUX_CUDA(cudaStreamSynchronize(E->copy_stream));
+        return LUX_OK;
+    }
     LUX_CUDA(cudaMemcpyAsync(rgb, j.image, bytes, cudaMemcpyDeviceToHost, E->stream));
     LUX_CUDA(cudaStreamSynchronize(E->stream));
     return LUX_OK;
@@ -741,6 +800,13 @@ int lux_engine_free(lux_engine* E) {
     if (E->ctr_h) cudaFreeHost(E->ctr_h);
     for (cudaEvent_t e : E->ev)
         if (e) cudaEventDestroy(e);
+    for (auto& pe : E->step_ev)
+        for (cudaEvent_t e : pe)
+            if (e) cudaEventDestroy(e);
+    if (E->copy_stream) {
+        cudaStreamSynchronize(E->copy_stream);
+        cudaStreamDestroy(E->copy_stream);
+    }
     if (E->stream) cudaStreamDestroy(E->stream);
     delete E;
     return LUX_OK;
