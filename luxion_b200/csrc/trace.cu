@@ -52,7 +52,7 @@ constexpr uint32_t kRecMask = 0xffu;
 // fewer lanes than this with triangles to test: push the triangle groups and keep
 // traversing nodes (the postponement of Ylitie et al. 2017); 6 and a refill threshold of 20
 // lanes were the fastest of the values tried on the 1M-triangle 1080p workload (3, 4 and 6;
-// 16, 20, 22, 24 and 28), and 24 for the occlusion rays (16, 20 and 24)
+// 16, 18, 20, 22, 24 and 28), and 24 for the occlusion rays (16, 20, 24, 28 and 32)
 constexpr int kPostpone = 6;
 // Slab acceptance tnear <= tfar * kWiden (tnear >= 0): a relative margin of 2^-17, far above
 // the few-ulp rounding of the plane distances.
